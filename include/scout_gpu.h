@@ -1,0 +1,178 @@
+/*
+ * scout_gpu.h -- device C ABI of scout-b200 (sm_100a).
+ *
+ * The reference keeps its kernels static inside each src/<problem>/scout_<problem>.cu and
+ * drives them from main(); it has no library interface. This header is the seam the
+ * host side (bin/scout_<problem>, the Python package, or a foreign caller over ctypes/cgo)
+ * binds. Each entry point names the reference code it replaces (path:line inside the
+ * reference project, anonymous-artifacts/SCOUT).
+ *
+ * Conventions
+ *  - Every function returns SCOUT_OK (0) or a negative SCOUT_E* code and never exits the
+ *    process (the reference calls exit(1) on any CUDA error, core/gpu_common.h:12-19).
+ *    scout_last_error(ctx) returns the message of the last failure on that context
+ *    (scout_last_error(NULL): last failure of scout_ctx_create on this thread).
+ *  - Vertex ids are 0-indexed int32; adjacency offsets are int64.
+ *  - Host buffers passed in are only read or written during the call; they may be pageable.
+ *  - One controlling host thread per context. Contexts are independent (replicas).
+ *  - No call drops work silently: a capacity overflow grows the buffer (within the HBM
+ *    budget) or returns SCOUT_E_CAPACITY (the reference truncates and warns,
+ *    scout_bfs.cu:186-193, 242; scout_coloring.cu:180-188).
+ */
+#ifndef SCOUT_GPU_H
+#define SCOUT_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCOUT_OK          0
+#define SCOUT_E_INVALID  (-1)  /* bad argument or id out of range            */
+#define SCOUT_E_CUDA     (-2)  /* CUDA runtime error                          */
+#define SCOUT_E_CAPACITY (-3)  /* buffer too small or HBM budget exceeded     */
+#define SCOUT_E_TIMEOUT  (-4)  /* a bounded device-side wait expired          */
+#define SCOUT_E_STATE    (-5)  /* call out of order (e.g. repair before seal) */
+#define SCOUT_E_IO       (-6)  /* file could not be opened / read / written   */
+#define SCOUT_E_FORMAT   (-7)  /* malformed .egr or state file                */
+#define SCOUT_E_NODEV    (-8)  /* no CUDA device                              */
+
+enum scout_problem { SCOUT_MIS = 0, SCOUT_COLORING = 1, SCOUT_BFS = 2, SCOUT_CC = 3 };
+
+/* Per-edit operation. TOGGLE is the reference batch-file semantics: insert if (u,v) is
+ * absent from the graph as it stood before this batch, delete if present
+ * (core/cli_setup.h:87-103); a pair toggled twice in one batch is classified twice against
+ * that same state. INSERT/DELETE carry a classification made by the caller (the MIS binary
+ * classifies every batch against the base graph up front, scout_mis.cu:835-842) and are
+ * applied only when consistent with the current graph (scout_mis.cu:743-749). */
+enum scout_op { SCOUT_OP_TOGGLE = 0, SCOUT_OP_INSERT = 1, SCOUT_OP_DELETE = 2 };
+
+typedef struct scout_edge { int32_t u; int32_t v; } scout_edge;
+
+enum scout_policy   { SCOUT_SCHED_PLAIN = 0, SCOUT_SCHED_LEARNED = 1 };
+enum scout_mode     { SCOUT_MODE_AUTO = 0, SCOUT_MODE_INCREMENTAL = 1, SCOUT_MODE_RECOMPUTE = 2 };
+enum scout_frontier { SCOUT_FRONTIER_AUTO = 0, SCOUT_FRONTIER_QUEUE = 1, SCOUT_FRONTIER_BITMAP = 2 };
+
+/* Scheduling knobs. A zeroed struct (or NULL) is the plain engine with the reference's
+ * heuristics: CC search bound 5000, or unbounded below average degree 10
+ * (scout_cc.cu:68-69, 469; core/local_repair.h:13-20). */
+typedef struct scout_sched {
+    int32_t policy;           /* scout_policy                                       */
+    int32_t mode;             /* scout_mode: incremental repair vs full recompute    */
+    int32_t frontier;         /* scout_frontier                                     */
+    int32_t lanes_per_vertex; /* 0 auto; else 1, 2, 4, 8, 32                         */
+    int64_t search_bound;     /* CC local-search bound (vertices); 0 = reference rule */
+    int64_t reserved[4];
+} scout_sched;
+
+/* Per-batch statistics (the fields of the reference's Stats structs, scout_bfs.cu:417-424,
+ * scout_cc.cu:344-352, scout_coloring.cu:160-165, plus device timings and traffic). */
+typedef struct scout_batch_stats {
+    int64_t edits;        /* edits accepted                                         */
+    int64_t insertions;   /* classified as insertions                                */
+    int64_t deletions;    /* classified as deletions                                 */
+    int64_t noop;         /* edits that needed no repair                             */
+    int64_t conflicts;    /* coloring: same-colour insertions; MIS: both-in-set inserts */
+    int64_t affected;     /* vertices examined by the repair                         */
+    int64_t changed;      /* solution entries whose value changed                    */
+    int64_t rounds;       /* device repair rounds                                    */
+    int64_t recomputes;   /* full on-GPU recomputes taken                            */
+    int64_t splits;       /* CC: components split by a local search                  */
+    int64_t searches;     /* CC: local searches run                                  */
+    int64_t hbm_bytes;    /* algorithmic HBM bytes of the repair kernels              */
+    int64_t h2d_bytes;    /* host-to-device bytes of the call                         */
+    int64_t d2h_bytes;    /* device-to-host bytes of the call                         */
+    double  ms_update;    /* device: classification + merge of the edits into HBM rows */
+    double  ms_repair;    /* device: repair kernels                                  */
+    double  ms_commit;    /* device: changed-entry gather + copy back                */
+    double  ms_total;     /* host wall time of the call                              */
+    int64_t update_bytes; /* algorithmic HBM bytes of the row merge                   */
+    int64_t reserved[7];
+} scout_batch_stats;
+
+typedef struct scout_ctx scout_ctx;
+
+/* ---- context ------------------------------------------------------------------------ */
+/* Replaces gpu_warmup_and_device_setup (core/cli_setup.h:54-58): selects the device,
+ * creates the context's streams and events. hbm_budget_bytes caps every allocation the
+ * context makes (0 = 90% of the device's free memory); the reference has no such knob. */
+int scout_ctx_create(int device, uint64_t hbm_budget_bytes, scout_ctx** out);
+int scout_ctx_destroy(scout_ctx* ctx);
+const char* scout_last_error(const scout_ctx* ctx);
+int scout_device_count(int* out);
+/* Device name and HBM bytes currently held by the context. */
+int scout_ctx_info(scout_ctx* ctx, char* name, int name_cap, uint64_t* bytes_held);
+
+/* ---- graph store in HBM ------------------------------------------------------------- */
+/* Sizes the row table for n vertices and the element pool for nnz entries plus headroom
+ * for rows rewritten by later batches (alloc_pair / alloc_and_upload, gpu_common.h:43-72). */
+int scout_graph_reserve(scout_ctx* ctx, int64_t n, int64_t nnz);
+/* Gather of rows from host staging into HBM: nrows rows (ids[i], elements
+ * elems[offs[i] .. offs[i+1]) ) are copied to the device pool and become the current
+ * adjacency of those vertices. Replaces the pack + cudaMemcpyAsync of every round
+ * (scout_bfs.cu:207-229, scout_coloring.cu:177-201, scout_mis.cu:583-647) and the chunked
+ * full-graph upload (scout_cc.cu:160-215). slot (0 or 1) selects the copy stream and the
+ * pinned bounce slab; a slot's previous copy is waited for before its slab is reused. */
+int scout_stage_rows(scout_ctx* ctx, int slot, const int32_t* ids, const int64_t* offs,
+                     const int32_t* elems, int64_t nrows, int64_t nelems);
+/* Ends staging: waits for both slots, sorts any row that is not ascending, and makes the
+ * store ready for repairs. */
+int scout_graph_seal(scout_ctx* ctx);
+/* reserve + one stage of every row + seal, from a host CSR. */
+int scout_graph_load_csr(scout_ctx* ctx, int64_t n, const int64_t* off, const int32_t* adj);
+int scout_graph_info(scout_ctx* ctx, int64_t* n, int64_t* nnz, int64_t* pool_used,
+                     int64_t* pool_cap);
+/* Current adjacency, rows ascending, written as CSR (off: n+1 entries). Two-call protocol:
+ * with cap < nnz returns SCOUT_E_CAPACITY and stores nnz in off[n]. */
+int scout_graph_download(scout_ctx* ctx, int64_t* off, int32_t* adj, int64_t cap);
+/* Rewrites the pool so every row is contiguous again (the on-device half of
+ * compact_flash_graph, core/flash_compactor.h:23-119). */
+int scout_graph_compact(scout_ctx* ctx);
+/* Toggle classification only (cli_setup.h:98 / FlashGraph.h:356-366) against the current
+ * HBM adjacency: is_insertion[i] = 1 if (u,v) is absent. */
+int scout_classify(scout_ctx* ctx, const scout_edge* e, int64_t m, uint8_t* is_insertion);
+
+/* ---- solution state ----------------------------------------------------------------- */
+/* Upload / download of the maintained solution (setMISFromHost / getMISToHost,
+ * scout_mis.cu:480-494; the level/colour cudaMemcpy of scout_bfs.cu:562,
+ * scout_coloring.cu:313). Layouts: MIS 0/1 flags, coloring colours, BFS levels (-1
+ * unreached), CC component labels (any labelling; the store keeps min-vertex-id labels). */
+int scout_state_upload(scout_ctx* ctx, int problem, const int32_t* sol, int64_t n);
+int scout_state_download(scout_ctx* ctx, int problem, int32_t* out, int64_t n);
+/* BFS source vertex (the reference fixes it to 0, scout_bfs.cu:547). */
+int scout_set_source(scout_ctx* ctx, int32_t source);
+
+/* ---- repair --------------------------------------------------------------------------- */
+/* One batch: edits go to the device, are classified (ops == NULL means all TOGGLE),
+ * merged into the HBM rows, and the solution is repaired on the device. Returns when the
+ * batch is repaired. Replaces processBatch of each engine: scout_mis.cu:738-767 (launch +
+ * collect), scout_coloring.cu:243-277, scout_bfs.cu:436-515, scout_cc.cu:392-441. */
+int scout_repair(scout_ctx* ctx, int problem, const scout_edge* edits, const uint8_t* ops,
+                 int64_t m, const scout_sched* sched, scout_batch_stats* stats);
+int scout_repair_mis(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                     const scout_sched* sched, scout_batch_stats* stats);
+int scout_repair_coloring(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops,
+                          int64_t m, const scout_sched* sched, scout_batch_stats* stats);
+int scout_repair_bfs(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                     const scout_sched* sched, scout_batch_stats* stats);
+int scout_repair_cc(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                    const scout_sched* sched, scout_batch_stats* stats);
+/* Commit of the last repair's changed entries into a host mirror of n entries: the device
+ * gathers (id, value) pairs of changed entries and copies them back; the host scatters
+ * them. Replaces the gather_levels + D2H + mirror loop (scout_bfs.cu:244-262), the proposal
+ * fold-back (scout_coloring.cu:215-219) and getMISToHost (scout_mis.cu:487-494). */
+int scout_commit(scout_ctx* ctx, int problem, int32_t* host_mirror, int64_t n,
+                 int64_t* changed_count);
+/* Full on-GPU recomputes: BFS from source (gpu_full_bfs, scout_bfs.cu:274-323) and
+ * min-id components (full_recompute_cc_gpu, scout_cc.cu:118-278). */
+int scout_recompute_bfs(scout_ctx* ctx, int32_t source, scout_batch_stats* stats);
+int scout_recompute_cc(scout_ctx* ctx, scout_batch_stats* stats);
+/* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
+int scout_sync(scout_ctx* ctx, int64_t timeout_us);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCOUT_GPU_H */

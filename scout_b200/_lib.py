@@ -1,0 +1,131 @@
+"""ctypes bindings of include/scout_gpu.h and include/scout_host.h (libscout.so).
+
+The library is built in-tree by ``python -m scout_b200.build``; importing this module
+without it raises immediately (there is no fallback implementation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libscout.so")
+
+SCOUT_OK = 0
+ERRORS = {
+    -1: "SCOUT_E_INVALID", -2: "SCOUT_E_CUDA", -3: "SCOUT_E_CAPACITY", -4: "SCOUT_E_TIMEOUT",
+    -5: "SCOUT_E_STATE", -6: "SCOUT_E_IO", -7: "SCOUT_E_FORMAT", -8: "SCOUT_E_NODEV",
+}
+PROBLEMS = {"mis": 0, "coloring": 1, "bfs": 2, "cc": 3}
+OP_TOGGLE, OP_INSERT, OP_DELETE = 0, 1, 2
+STREAM_MIXED, STREAM_PREFERENTIAL, STREAM_LOWDEG = 0, 1, 2
+
+
+class ScoutEdge(C.Structure):
+    _fields_ = [("u", C.c_int32), ("v", C.c_int32)]
+
+
+class ScoutSched(C.Structure):
+    _fields_ = [("policy", C.c_int32), ("mode", C.c_int32), ("frontier", C.c_int32),
+                ("lanes_per_vertex", C.c_int32), ("search_bound", C.c_int64), ("reserved", C.c_int64 * 4)]
+
+
+class ScoutBatchStats(C.Structure):
+    _fields_ = [("edits", C.c_int64), ("insertions", C.c_int64), ("deletions", C.c_int64),
+                ("noop", C.c_int64), ("conflicts", C.c_int64), ("affected", C.c_int64),
+                ("changed", C.c_int64), ("rounds", C.c_int64), ("recomputes", C.c_int64),
+                ("splits", C.c_int64), ("searches", C.c_int64), ("hbm_bytes", C.c_int64),
+                ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("ms_update", C.c_double),
+                ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
+                ("update_bytes", C.c_int64), ("reserved", C.c_int64 * 7)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+_vp = C.c_void_p
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u8p = C.POINTER(C.c_uint8)
+_edgep = C.POINTER(ScoutEdge)
+
+# (name, restype, argtypes) for every symbol the two headers declare.
+SIGNATURES = [
+    # scout_gpu.h
+    ("scout_ctx_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    ("scout_ctx_destroy", C.c_int, [_vp]),
+    ("scout_last_error", C.c_char_p, [_vp]),
+    ("scout_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("scout_ctx_info", C.c_int, [_vp, C.c_char_p, C.c_int, C.POINTER(C.c_uint64)]),
+    ("scout_graph_reserve", C.c_int, [_vp, C.c_int64, C.c_int64]),
+    ("scout_stage_rows", C.c_int, [_vp, C.c_int, _i32p, _i64p, _i32p, C.c_int64, C.c_int64]),
+    ("scout_graph_seal", C.c_int, [_vp]),
+    ("scout_graph_load_csr", C.c_int, [_vp, C.c_int64, _i64p, _i32p]),
+    ("scout_graph_info", C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
+    ("scout_graph_download", C.c_int, [_vp, _i64p, _i32p, C.c_int64]),
+    ("scout_graph_compact", C.c_int, [_vp]),
+    ("scout_classify", C.c_int, [_vp, _edgep, C.c_int64, _u8p]),
+    ("scout_state_upload", C.c_int, [_vp, C.c_int, _i32p, C.c_int64]),
+    ("scout_state_download", C.c_int, [_vp, C.c_int, _i32p, C.c_int64]),
+    ("scout_set_source", C.c_int, [_vp, C.c_int32]),
+    ("scout_repair", C.c_int, [_vp, C.c_int, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched),
+                               C.POINTER(ScoutBatchStats)]),
+    ("scout_repair_mis", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_repair_coloring", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched),
+                                        C.POINTER(ScoutBatchStats)]),
+    ("scout_repair_bfs", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_repair_cc", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_commit", C.c_int, [_vp, C.c_int, _i32p, C.c_int64, _i64p]),
+    ("scout_recompute_bfs", C.c_int, [_vp, C.c_int32, C.POINTER(ScoutBatchStats)]),
+    ("scout_recompute_cc", C.c_int, [_vp, C.POINTER(ScoutBatchStats)]),
+    ("scout_sync", C.c_int, [_vp, C.c_int64]),
+    # scout_host.h
+    ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    ("scout_egr_close", C.c_int, [_vp]),
+    ("scout_egr_nodes", C.c_int64, [_vp]),
+    ("scout_egr_edges", C.c_int64, [_vp]),
+    ("scout_egr_is_wide", C.c_int, [_vp]),
+    ("scout_egr_offsets", C.c_int, [_vp, _i64p]),
+    ("scout_egr_nlist", _i32p, [_vp]),
+    ("scout_egr_write", C.c_int, [C.c_char_p, C.c_int64, _i64p, _i32p, C.c_int]),
+    ("scout_hgraph_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    ("scout_hgraph_close", C.c_int, [_vp]),
+    ("scout_hgraph_nodes", C.c_int64, [_vp]),
+    ("scout_hgraph_is_adjacent", C.c_int, [_vp, C.c_int32, C.c_int32]),
+    ("scout_hgraph_insert", C.c_int, [_vp, C.c_int32, C.c_int32]),
+    ("scout_hgraph_remove", C.c_int, [_vp, C.c_int32, C.c_int32]),
+    ("scout_hgraph_degree", C.c_int64, [_vp, C.c_int32]),
+    ("scout_hgraph_neighbors", C.c_int64, [_vp, C.c_int32, _i32p, C.c_int64]),
+    ("scout_hgraph_delta_edits", C.c_int64, [_vp]),
+    ("scout_hgraph_compact", C.c_int, [_vp, C.c_char_p]),
+    ("scout_fetch_all", C.c_int, [_vp, _vp, C.c_int64]),
+    ("scout_fetch_rows", C.c_int, [_vp, _vp, _i32p, C.c_int64]),
+    ("scout_parse_batch_file", C.c_int, [C.c_char_p, C.c_int64, _edgep, C.c_int64, _i64p]),
+    ("scout_read_ints", C.c_int, [C.c_char_p, _i64p, C.c_int64, _i64p]),
+    ("scout_load_state", C.c_int, [C.c_char_p, C.c_int, C.c_int64, _i32p, _i64p]),
+    ("scout_write_state", C.c_int, [C.c_char_p, C.c_int, C.c_int64, _i32p]),
+    ("scout_write_batch_folder", C.c_int, [C.c_char_p, _edgep, C.c_int64, C.c_int64]),
+    ("scout_gen_rmat", C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(_vp)]),
+    ("scout_csr_from_arrays", C.c_int, [C.c_int64, _i64p, _i32p, C.POINTER(_vp)]),
+    ("scout_csr_free", C.c_int, [_vp]),
+    ("scout_csr_nodes", C.c_int64, [_vp]),
+    ("scout_csr_nnz", C.c_int64, [_vp]),
+    ("scout_csr_offsets", _i64p, [_vp]),
+    ("scout_csr_adj", _i32p, [_vp]),
+    ("scout_gen_stream", C.c_int, [_vp, C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, _edgep]),
+    ("scout_init_state", C.c_int, [_vp, C.c_int, C.c_int32, _i32p]),
+]
+
+
+def load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build the CUDA extension with `python -m scout_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = load()

@@ -1,0 +1,398 @@
+// api.cu -- the C ABI of scout_gpu.h: context, graph store, state, repair dispatch, commit.
+#include "ctx.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+namespace scout {
+
+int host_fail(int code, const std::string& msg);   // graph_host.cpp (thread-local message)
+const char* host_last_error();
+
+int cuda_fail(scout_ctx* c, cudaError_t e, const char* where) {
+    std::string msg = std::string(where) + ": " + cudaGetErrorString(e);
+    if (c) c->err = msg;
+    else host_fail(SCOUT_E_CUDA, msg);
+    return SCOUT_E_CUDA;
+}
+
+int dev_alloc(scout_ctx* c, void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 256;
+    if (c->held + bytes > c->budget)
+        return c->fail(SCOUT_E_CAPACITY, std::string("HBM budget exceeded allocating ") + what + " (" +
+                                             std::to_string(bytes) + " B, held " + std::to_string(c->held) +
+                                             " of " + std::to_string(c->budget) + ")");
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return c->fail(e == cudaErrorMemoryAllocation ? SCOUT_E_CAPACITY : SCOUT_E_CUDA,
+                       std::string("cudaMalloc failed for ") + what + ": " + cudaGetErrorString(e));
+    }
+    c->held += bytes;
+    return SCOUT_OK;
+}
+
+void dev_free(scout_ctx* c, void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    if (bytes == 0) bytes = 256;
+    c->held -= std::min<uint64_t>(c->held, bytes);
+}
+
+int pin_grow(scout_ctx* c, void** p, int64_t* cap, int64_t need) {
+    if (*p && *cap >= need) return SCOUT_OK;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    int64_t nc = need + need / 4 + 4096;
+    SCOUT_CU(c, cudaMallocHost(p, (size_t)nc));
+    *cap = nc;
+    return SCOUT_OK;
+}
+
+int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem) {
+    int per_sm = 0;
+    SCOUT_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    if (per_sm < 1) return c->fail(SCOUT_E_CUDA, "persistent kernel does not fit on an SM");
+    per_sm = std::min(per_sm, 4);
+    dim3 grid((unsigned)(per_sm * c->sm_count)), block((unsigned)threads);
+    SCOUT_CU(c, cudaLaunchCooperativeKernel(fn, grid, block, args, smem, c->s_main));
+    return SCOUT_OK;
+}
+
+static void release(scout_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->s_main) cudaStreamSynchronize(c->s_main);
+    for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
+    void* devs[] = {c->row, c->pool, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c,
+                    c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
+                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_misc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
+                    c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
+    for (void* p : devs) if (p) cudaFree(p);
+    void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
+                     c->h_slab_off[0], c->h_slab_off[1], c->h_slab_ids[0], c->h_slab_ids[1]};
+    for (void* p : hosts) if (p) cudaFreeHost(p);
+    for (int i = 0; i < 6; i++) if (c->ev_t[i]) cudaEventDestroy(c->ev_t[i]);
+    for (int i = 0; i < 2; i++) {
+        if (c->ev_copy[i]) cudaEventDestroy(c->ev_copy[i]);
+        if (c->s_copy[i]) cudaStreamDestroy(c->s_copy[i]);
+    }
+    if (c->s_main) cudaStreamDestroy(c->s_main);
+    delete c;
+}
+
+static int32_t** state_slot(scout_ctx* c, int problem) {
+    switch (problem) {
+    case SCOUT_MIS: return &c->mis;
+    case SCOUT_COLORING: return &c->color;
+    case SCOUT_BFS: return &c->level;
+    case SCOUT_CC: return &c->label;
+    default: return nullptr;
+    }
+}
+
+__global__ void k_label_min(const int32_t* __restrict__ lab, int32_t* __restrict__ mn, int64_t n) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        atomicMin(&mn[lab[v]], (int32_t)v);
+}
+__global__ void k_label_apply(int32_t* __restrict__ lab, const int32_t* __restrict__ mn, int64_t n) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        lab[v] = mn[lab[v]];
+}
+__global__ void k_fill_i32(int32_t* __restrict__ a, int64_t n, int32_t x) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        a[v] = x;
+}
+
+// (id, value) pairs of the touched list for the commit.
+__global__ void k_commit_gather(const int32_t* __restrict__ list, const DevCounters* __restrict__ ctr,
+                                const int32_t* __restrict__ val, int32_t* __restrict__ out) {
+    const int cnt = ctr->changed;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int32_t v = list[i];
+        out[2 * i] = v;
+        out[2 * i + 1] = val[v];
+    }
+}
+
+static double ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { cudaGetLastError(); return 0.0; }
+    return (double)ms;
+}
+
+}  // namespace scout
+
+using namespace scout;
+
+extern "C" {
+
+const char* scout_last_error(const scout_ctx* c) { return c ? c->err.c_str() : host_last_error(); }
+
+int scout_device_count(int* out) {
+    if (!out) return SCOUT_E_INVALID;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { cudaGetLastError(); n = 0; }
+    *out = n;
+    return SCOUT_OK;
+}
+
+int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
+    if (!out) return host_fail(SCOUT_E_INVALID, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return host_fail(SCOUT_E_NODEV, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return host_fail(SCOUT_E_INVALID, "device id out of range");
+    auto* c = new scout_ctx();
+    c->device = device;
+    // gpu_warmup_and_device_setup (cli_setup.h:54-58)
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaFree(0);
+    cudaDeviceProp prop;
+    if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) { release(c); return cuda_fail(nullptr, e, "device setup"); }
+    std::strncpy(c->name, prop.name, sizeof(c->name) - 1);
+    c->sm_count = prop.multiProcessorCount;
+    if (!prop.cooperativeLaunch) { release(c); return host_fail(SCOUT_E_NODEV, "device lacks cooperative launch"); }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = budget ? budget : (uint64_t)(0.9 * (double)fr);
+    bool ok = cudaStreamCreateWithFlags(&c->s_main, cudaStreamNonBlocking) == cudaSuccess;
+    for (int i = 0; i < 2 && ok; i++) {
+        ok = cudaStreamCreateWithFlags(&c->s_copy[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->ev_copy[i], cudaEventDisableTiming) == cudaSuccess;
+    }
+    for (int i = 0; i < 6 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
+    ok = ok && cudaMallocHost((void**)&c->h_ctr, sizeof(DevCounters)) == cudaSuccess &&
+         cudaMallocHost((void**)&c->h_bar, sizeof(GridBar)) == cudaSuccess;
+    if (!ok) { cudaError_t le = cudaGetLastError(); release(c); return cuda_fail(nullptr, le, "context streams"); }
+    int rc = dev_alloc(c, (void**)&c->d_ctr, sizeof(DevCounters), "counters");
+    if (rc == SCOUT_OK) rc = dev_alloc(c, (void**)&c->d_bar, sizeof(GridBar), "grid barrier");
+    if (rc == SCOUT_OK) rc = dev_alloc(c, (void**)&c->d_flags, 64, "error flags");
+    if (rc != SCOUT_OK) { std::string m = c->err; release(c); return host_fail(rc, m); }
+    cudaMemset(c->d_ctr, 0, sizeof(DevCounters));
+    cudaMemset(c->d_bar, 0, sizeof(GridBar));
+    cudaMemset(c->d_flags, 0, 64);
+    *out = c;
+    return SCOUT_OK;
+}
+
+int scout_ctx_destroy(scout_ctx* c) { release(c); return SCOUT_OK; }
+
+int scout_ctx_info(scout_ctx* c, char* name, int cap, uint64_t* held) {
+    if (!c) return SCOUT_E_INVALID;
+    if (name && cap > 0) { std::strncpy(name, c->name, (size_t)cap - 1); name[cap - 1] = 0; }
+    if (held) *held = c->held;
+    return SCOUT_OK;
+}
+
+// ---- state -------------------------------------------------------------------------------
+int scout_state_upload(scout_ctx* c, int problem, const int32_t* sol, int64_t n) {
+    if (!c || !sol) return SCOUT_E_INVALID;
+    int32_t** slot = state_slot(c, problem);
+    if (!slot) return c->fail(SCOUT_E_INVALID, "unknown problem");
+    if (!c->reserved || n != c->n) return c->fail(SCOUT_E_STATE, "state size does not match the graph");
+    if (problem == SCOUT_CC)
+        for (int64_t v = 0; v < n; v++)
+            if (sol[v] < 0 || sol[v] >= n) return c->fail(SCOUT_E_INVALID, "component labels must lie in [0, n)");
+    cudaSetDevice(c->device);
+    if (!*slot) SCOUT_RC(dev_alloc(c, (void**)slot, (size_t)n * 4, "solution state"));
+    SCOUT_CU(c, cudaMemcpyAsync(*slot, sol, (size_t)n * 4, cudaMemcpyHostToDevice, c->s_main));
+    if (problem == SCOUT_CC) {   // min-vertex-id labels
+        SCOUT_RC(graph_ensure_scratch(c));
+        k_fill_i32<<<blocks_for(n, 256), 256, 0, c->s_main>>>(c->aux_v, n, INT32_MAX);
+        k_label_min<<<blocks_for(n, 256), 256, 0, c->s_main>>>(*slot, c->aux_v, n);
+        k_label_apply<<<blocks_for(n, 256), 256, 0, c->s_main>>>(*slot, c->aux_v, n);
+        SCOUT_LAUNCH(c, "label canonicalisation");
+    }
+    SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+    return SCOUT_OK;
+}
+
+int scout_state_download(scout_ctx* c, int problem, int32_t* out, int64_t n) {
+    if (!c || !out) return SCOUT_E_INVALID;
+    int32_t** slot = state_slot(c, problem);
+    if (!slot) return c->fail(SCOUT_E_INVALID, "unknown problem");
+    if (!*slot || n != c->n) return c->fail(SCOUT_E_STATE, "no state uploaded for this problem");
+    cudaSetDevice(c->device);
+    SCOUT_CU(c, cudaMemcpyAsync(out, *slot, (size_t)n * 4, cudaMemcpyDeviceToHost, c->s_main));
+    SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+    return SCOUT_OK;
+}
+
+int scout_set_source(scout_ctx* c, int32_t s) {
+    if (!c) return SCOUT_E_INVALID;
+    if (s < 0 || (c->reserved && s >= c->n)) return c->fail(SCOUT_E_INVALID, "source out of range");
+    c->source = s;
+    return SCOUT_OK;
+}
+
+// ---- repair ------------------------------------------------------------------------------
+int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                 const scout_sched* sched, scout_batch_stats* st) {
+    if (!c || m < 0 || (m > 0 && !edits)) return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
+    if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
+    int32_t** slot = state_slot(c, problem);
+    if (!slot) return c->fail(SCOUT_E_INVALID, "unknown problem");
+    if (!*slot) return c->fail(SCOUT_E_STATE, "no state uploaded for this problem");
+    cudaSetDevice(c->device);
+    auto t0 = std::chrono::steady_clock::now();
+    scout_batch_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    scout_sched sd;
+    std::memset(&sd, 0, sizeof(sd));
+    if (sched) sd = *sched;
+    c->last_problem = problem;
+    SCOUT_RC(batch_begin(c));
+    SCOUT_RC(lists_ensure(c));
+    c->epoch++;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[0], c->s_main));
+    SCOUT_RC(graph_update(c, edits, ops, m, st));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[1], c->s_main));
+    int rc = SCOUT_OK;
+    switch (problem) {
+    case SCOUT_BFS: rc = bfs_repair(c, st); break;
+    case SCOUT_CC: rc = cc_repair(c, &sd, st); break;
+    case SCOUT_COLORING: rc = coloring_repair(c, st); break;
+    case SCOUT_MIS: rc = mis_repair(c, st); break;
+    }
+    if (rc != SCOUT_OK) return rc;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
+    SCOUT_RC(counters_fetch(c));
+    const DevCounters& h = *c->h_ctr;
+    c->tail += h.new_elems;
+    c->nnz += h.nnz_delta;
+    c->qtag += (uint32_t)h.rounds + 8;
+    st->edits = h.n_ins + h.n_del;
+    st->insertions = h.n_ins;
+    st->deletions = h.n_del;
+    st->noop = h.noop;
+    st->conflicts = h.conflicts;
+    st->affected = h.affected;
+    st->changed = h.changed;
+    st->rounds = h.rounds;
+    st->recomputes += h.recomputes;
+    st->splits = h.splits;
+    st->searches = h.searches;
+    st->hbm_bytes = h.hbm_bytes;
+    st->update_bytes = h.update_bytes;
+    st->d2h_bytes += sizeof(DevCounters);
+    st->ms_update = ev_ms(c->ev_t[0], c->ev_t[1]);
+    st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
+    c->last_changed = h.changed;
+    st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SCOUT_OK;
+}
+
+int scout_repair_mis(scout_ctx* c, const scout_edge* e, const uint8_t* o, int64_t m, const scout_sched* s, scout_batch_stats* st) { return scout_repair(c, SCOUT_MIS, e, o, m, s, st); }
+int scout_repair_coloring(scout_ctx* c, const scout_edge* e, const uint8_t* o, int64_t m, const scout_sched* s, scout_batch_stats* st) { return scout_repair(c, SCOUT_COLORING, e, o, m, s, st); }
+int scout_repair_bfs(scout_ctx* c, const scout_edge* e, const uint8_t* o, int64_t m, const scout_sched* s, scout_batch_stats* st) { return scout_repair(c, SCOUT_BFS, e, o, m, s, st); }
+int scout_repair_cc(scout_ctx* c, const scout_edge* e, const uint8_t* o, int64_t m, const scout_sched* s, scout_batch_stats* st) { return scout_repair(c, SCOUT_CC, e, o, m, s, st); }
+
+int scout_commit(scout_ctx* c, int problem, int32_t* mirror, int64_t n, int64_t* changed) {
+    if (!c || !mirror) return SCOUT_E_INVALID;
+    int32_t** slot = state_slot(c, problem);
+    if (!slot || !*slot || n != c->n) return c->fail(SCOUT_E_STATE, "nothing to commit for this problem");
+    if (problem != c->last_problem) return c->fail(SCOUT_E_STATE, "the last repair was for another problem");
+    cudaSetDevice(c->device);
+    int64_t cnt = c->last_changed;
+    int64_t diff = 0;
+    if (cnt > 0) {
+        SCOUT_RC(pin_grow(c, &c->h_pin_commit, &c->cap_pin_commit, cnt * 8));
+        k_commit_gather<<<blocks_for(cnt, 256), 256, 0, c->s_main>>>(c->d_list[0], c->d_ctr, *slot, c->d_commit);
+        SCOUT_LAUNCH(c, "k_commit_gather");
+        SCOUT_CU(c, cudaMemcpyAsync(c->h_pin_commit, c->d_commit, (size_t)cnt * 8, cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        const int32_t* p = (const int32_t*)c->h_pin_commit;
+        for (int64_t i = 0; i < cnt; i++) {
+            int32_t v = p[2 * i], x = p[2 * i + 1];
+            if (v < 0 || v >= n) continue;
+            if (mirror[v] != x) { mirror[v] = x; diff++; }
+        }
+    }
+    if (changed) *changed = diff;
+    c->last_changed = 0;
+    return SCOUT_OK;
+}
+
+int scout_recompute_bfs(scout_ctx* c, int32_t source, scout_batch_stats* st) {
+    if (!c) return SCOUT_E_INVALID;
+    if (!c->sealed || !c->level) return c->fail(SCOUT_E_STATE, "graph or BFS state missing");
+    if (source < 0 || source >= c->n) return c->fail(SCOUT_E_INVALID, "source out of range");
+    cudaSetDevice(c->device);
+    scout_batch_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    c->source = source;
+    c->last_problem = SCOUT_BFS;
+    SCOUT_RC(batch_begin(c));
+    SCOUT_RC(lists_ensure(c));
+    c->epoch++;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[1], c->s_main));
+    SCOUT_RC(bfs_recompute(c, source, st));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
+    SCOUT_RC(counters_fetch(c));
+    c->qtag += (uint32_t)c->h_ctr->rounds + 8;
+    st->rounds = c->h_ctr->rounds;
+    st->recomputes = 1;
+    st->hbm_bytes = c->h_ctr->hbm_bytes;
+    st->changed = c->h_ctr->changed;
+    c->last_changed = c->h_ctr->changed;
+    st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
+    return SCOUT_OK;
+}
+
+int scout_recompute_cc(scout_ctx* c, scout_batch_stats* st) {
+    if (!c) return SCOUT_E_INVALID;
+    if (!c->sealed || !c->label) return c->fail(SCOUT_E_STATE, "graph or CC state missing");
+    cudaSetDevice(c->device);
+    scout_batch_stats local;
+    if (!st) st = &local;
+    std::memset(st, 0, sizeof(*st));
+    c->last_problem = SCOUT_CC;
+    SCOUT_RC(batch_begin(c));
+    SCOUT_RC(lists_ensure(c));
+    c->epoch++;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[1], c->s_main));
+    SCOUT_RC(cc_recompute(c, st));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
+    SCOUT_RC(counters_fetch(c));
+    c->qtag += (uint32_t)c->h_ctr->rounds + 8;
+    st->rounds = c->h_ctr->rounds;
+    st->recomputes = 1;
+    st->hbm_bytes = c->h_ctr->hbm_bytes;
+    st->changed = c->h_ctr->changed;
+    c->last_changed = c->h_ctr->changed;
+    st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
+    return SCOUT_OK;
+}
+
+int scout_sync(scout_ctx* c, int64_t timeout_us) {
+    if (!c) return SCOUT_E_INVALID;
+    cudaSetDevice(c->device);
+    auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t ss[3] = {c->s_main, c->s_copy[0], c->s_copy[1]};
+    for (cudaStream_t s : ss) {
+        while (true) {
+            cudaError_t e = cudaStreamQuery(s);
+            if (e == cudaSuccess) break;
+            if (e != cudaErrorNotReady) return cuda_fail(c, e, "scout_sync");
+            if (timeout_us > 0 &&
+                std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count() > timeout_us)
+                return c->fail(SCOUT_E_TIMEOUT, "scout_sync timed out");
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+    return SCOUT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,355 @@
+// bfs.cu -- exact batch-dynamic BFS levels on the device (one persistent kernel per batch).
+//
+// Replaces the reference's per-edit host loop (processBatch, scout_bfs.cu:436-515), its
+// relax rounds (gpu_relax_round 177-272, relax_frontier_kernel 56-71), deletion cascade
+// (gpu_deletion_round 325-415, deletion_compute/apply 73-105) and full traversal
+// (gpu_full_bfs 274-323). The reference defers cascades past 200 touched vertices and can
+// leave stale levels until one catch-up traversal at the end of the stream; here every
+// batch ends with the exact BFS levels of the current graph:
+//   A  invalidate: a vertex at level l > 0 stays valid while some neighbour at level l - 1
+//      is valid; children (level l + 1) of every invalidated vertex are rechecked, so the
+//      fixpoint is exactly the set of vertices that lost every shortest-path parent.
+//   B  invalidated vertices restart at +inf and are seeded from their valid neighbours;
+//      inserted edges seed their endpoints (levels only ever decrease from here).
+//   C  relax rounds: atomicMin of level + 1 over the rows of every decreased vertex.
+// All three phases run in one cooperative launch separated by a bounded grid barrier; rows
+// longer than 1024 entries are split into 1024-entry chunks so a hub spreads over warps.
+#include "ctx.cuh"
+
+namespace scout {
+
+constexpr int BFS_THREADS = 256;
+constexpr int CHUNK = 1024;
+
+struct BfsParams {
+    DGraph g;
+    int32_t* level;
+    int32_t source;
+    const unsigned long long* hkeys;
+    int B;
+    unsigned long long* q[3];
+    int64_t qcap;
+    int32_t* inval;
+    int32_t* touched;
+    int32_t* st_inval;
+    int32_t* st_touch;
+    uint32_t* st_q;
+    int32_t epoch;
+    uint32_t qtag0;
+    DevCounters* ctr;
+    GridBar* bar;
+    int mode;   // 0 incremental, 1 full recompute from source
+};
+
+__device__ __forceinline__ int32_t ld_level(const int32_t* p) { return ld_volatile(p); }
+
+// Warp-cooperative push (all 32 lanes call): lanes with `pred` push vertex y into queue qn
+// once per round (tag), split into CHUNK-sized items; first touches of the batch are
+// appended to the touched list.
+__device__ __forceinline__ void push_vertex(const BfsParams& p, bool pred, int32_t y, int qi, uint32_t tag,
+                                            bool chunked, bool touch) {
+    bool first = false;
+    if (pred) first = atomicExch(&p.st_q[y], tag) != tag;
+    if (touch) {
+        bool nt = false;
+        if (pred) nt = atomicExch(&p.st_touch[y], p.epoch) != p.epoch;
+        int ti = warp_append(nt, &p.ctr->changed);
+        if (nt) p.touched[ti] = y;
+    }
+    int nit = 0;
+    if (first) {
+        if (chunked) {
+            int len = p.g.row[y].len;
+            nit = (len + CHUNK - 1) / CHUNK;
+        } else {
+            nit = 1;
+        }
+    }
+    int incl = warp_incl_scan_i(nit);
+    int tot = __shfl_sync(0xffffffffu, incl, WARP - 1);
+    if (tot == 0) return;
+    int base = 0;
+    if (lane_id() == WARP - 1) base = atomicAdd(&p.ctr->q_count[qi], tot);
+    base = __shfl_sync(0xffffffffu, base, WARP - 1);
+    long long start = (long long)base + incl - nit;
+    for (int k = 0; k < nit; k++) {
+        long long pos = start + k;
+        if (pos < p.qcap) p.q[qi][pos] = ((unsigned long long)k << 32) | (uint32_t)y;
+        else atomicExch(&p.ctr->overflow, 1);
+    }
+}
+
+__device__ __forceinline__ int qcount(const BfsParams& p, int qi) {
+    int c = ld_volatile(&p.ctr->q_count[qi]);
+    return (long long)c > p.qcap ? (int)p.qcap : c;
+}
+
+// One relax round over queue `cur` into `nxt` (warp-level load-balanced expansion).
+__device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, long long& bytes) {
+    const int cnt = qcount(p, cur);
+    const int W = gwarp_count();
+    for (long long gbase = (long long)gwarp_id() * WARP; gbase < cnt; gbase += (long long)W * WARP) {
+        long long idx = gbase + lane_id();
+        bool valid = idx < cnt;
+        unsigned long long item = valid ? p.q[cur][idx] : 0ull;
+        int32_t v = (int32_t)(item & 0xffffffffu);
+        int chunk = (int)(item >> 32);
+        long long s = 0;
+        int len = 0, lv = -1;
+        if (valid) {
+            Row r = p.g.row[v];
+            s = r.start + (long long)chunk * CHUNK;
+            len = min(CHUNK, r.len - chunk * CHUNK);
+            if (len < 0) len = 0;
+            lv = ld_level(p.level + v);
+            if (lv < 0) len = 0;
+        }
+        int incl = warp_incl_scan_i(len);
+        int total = __shfl_sync(0xffffffffu, incl, WARP - 1);
+        int excl = incl - len;
+        bytes += (long long)len * 8 + (valid ? 24 : 0);
+        for (int e0 = 0; e0 < total; e0 += WARP) {
+            int e = e0 + (int)lane_id();
+            int lo = 0, hi = WARP - 1;
+#pragma unroll
+            for (int it = 0; it < 5; it++) {
+                int mid = (lo + hi + 1) >> 1;
+                int em = __shfl_sync(0xffffffffu, excl, mid);
+                if (em <= e) lo = mid; else hi = mid - 1;
+            }
+            long long so = __shfl_sync(0xffffffffu, s, lo);
+            int eo = __shfl_sync(0xffffffffu, excl, lo);
+            int lo_lv = __shfl_sync(0xffffffffu, lv, lo);
+            bool dec = false;
+            int32_t y = 0;
+            if (e < total) {
+                y = p.g.pool[so + (e - eo)];
+                unsigned cand = (unsigned)(lo_lv + 1);
+                unsigned old = atomicMin((unsigned*)(p.level + y), cand);
+                dec = old > cand;
+            }
+            push_vertex(p, dec, y, nxt, tag, true, true);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
+    const int W = gwarp_count();
+    const int wid = gwarp_id();
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    long long bytes = 0;
+    int rounds = 0;
+    uint32_t tag = p.qtag0;
+    int cur = 0;
+
+    if (p.mode == 1) {
+        // Full recompute: every vertex restarts at +inf; all become touched.
+        for (int64_t v = tid; v < p.g.n; v += T) {
+            p.level[v] = v == p.source ? 0 : -1;
+            p.touched[v] = (int32_t)v;
+            p.st_touch[v] = p.epoch;
+        }
+        if (leader) {
+            p.ctr->changed = p.g.n;
+            int len = p.g.row[p.source].len;
+            int nit = (len + CHUNK - 1) / CHUNK;
+            for (int k = 0; k < nit; k++) p.q[0][k] = ((unsigned long long)k << 32) | (uint32_t)p.source;
+            p.ctr->q_count[0] = nit;
+            p.st_q[p.source] = tag;
+        }
+        if (tid == 0) bytes += (long long)p.g.n * 12;
+        if (!grid_sync(p.bar, 1)) return;
+    } else {
+        // ---- A: invalidation -------------------------------------------------------------
+        const int nh = ld_volatile(&p.ctr->n_half);
+        tag++;
+        for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
+            int64_t k = b + lane_id();
+            bool cand = false;
+            int32_t y = 0;
+            if (k < nh) {
+                unsigned long long key = p.hkeys[k];
+                int op = (int)((key >> p.B) & 1ull);
+                int32_t x = (int32_t)(key >> (p.B + 1));
+                y = (int32_t)(key & ((1ull << p.B) - 1));
+                if (op == 1) {
+                    int lx = ld_level(p.level + x), ly = ld_level(p.level + y);
+                    cand = lx >= 0 && ly == lx + 1;
+                }
+            }
+            push_vertex(p, cand, y, 0, tag, false, false);
+        }
+        if (!grid_sync(p.bar, 2)) return;
+        cur = 0;
+        while (true) {
+            const int cnt = qcount(p, cur);
+            if (cnt == 0) break;
+            const int nxt = (cur + 1) % 3, zer = (cur + 2) % 3;
+            if (leader) p.ctr->q_count[zer] = 0;
+            tag++;
+            for (int i = wid; i < cnt; i += W) {
+                int32_t c = (int32_t)(p.q[cur][i] & 0xffffffffu);
+                int lc = ld_level(p.level + c);
+                if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) continue;
+                Row r = p.g.row[c];
+                const int32_t* rw = p.g.pool + r.start;
+                bool found = false;
+                for (int b0 = 0; b0 < r.len && !found; b0 += WARP) {
+                    int k = b0 + (int)lane_id();
+                    bool ok = false;
+                    if (k < r.len) {
+                        int32_t w = rw[k];
+                        ok = ld_level(p.level + w) == lc - 1 && ld_volatile(p.st_inval + w) != p.epoch;
+                    }
+                    found = __any_sync(0xffffffffu, ok);
+                    if (k < r.len) bytes += 8;
+                }
+                if (found) continue;
+                if (lane_id() == 0) {
+                    p.st_inval[c] = p.epoch;
+                    int at = atomicAdd(&p.ctr->list_count[0], 1);
+                    p.inval[at] = c;
+                }
+                __syncwarp();
+                for (int b0 = 0; b0 < r.len; b0 += WARP) {
+                    int k = b0 + (int)lane_id();
+                    bool ch = false;
+                    int32_t w = 0;
+                    if (k < r.len) {
+                        w = rw[k];
+                        ch = ld_level(p.level + w) == lc + 1 && ld_volatile(p.st_inval + w) != p.epoch;
+                    }
+                    push_vertex(p, ch, w, nxt, tag, false, false);
+                }
+                if (lane_id() == 0) bytes += 8LL * r.len + 24;
+            }
+            rounds++;
+            if (!grid_sync(p.bar, 3)) return;
+            cur = nxt;
+        }
+        // ---- B: reset and seed --------------------------------------------------------------
+        const int ninv = ld_volatile(&p.ctr->list_count[0]);
+        for (int64_t b = tid - (tid & (WARP - 1)); b < ninv; b += T) {
+            int64_t i = b + lane_id();
+            bool ok = i < ninv;
+            int32_t c = ok ? p.inval[i] : 0;
+            bool nt = false;
+            if (ok) {
+                nt = atomicExch(&p.st_touch[c], p.epoch) != p.epoch;
+                p.level[c] = -1;
+            }
+            int ti = warp_append(nt, &p.ctr->changed);
+            if (nt) p.touched[ti] = c;
+        }
+        // all queues restart empty for phase C
+        if (!grid_sync(p.bar, 4)) return;
+        if (leader) { p.ctr->q_count[0] = 0; p.ctr->q_count[1] = 0; p.ctr->q_count[2] = 0; }
+        if (!grid_sync(p.bar, 5)) return;
+        tag++;
+        // boundary seeds: warp per invalidated vertex
+        for (int i = wid; i < ninv; i += W) {
+            int32_t c = p.inval[i];
+            Row r = p.g.row[c];
+            const int32_t* rw = p.g.pool + r.start;
+            unsigned best = 0xffffffffu;
+            for (int b0 = 0; b0 < r.len; b0 += WARP) {
+                int k = b0 + (int)lane_id();
+                if (k < r.len) {
+                    int32_t w = rw[k];
+                    if (ld_volatile(p.st_inval + w) != p.epoch) {
+                        int lw = ld_level(p.level + w);
+                        if (lw >= 0) best = min(best, (unsigned)lw);
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane_id() == 0) bytes += 8LL * r.len + 24;
+            bool dec = false;
+            if (lane_id() == 0 && best != 0xffffffffu) {
+                unsigned cand = best + 1;
+                unsigned old = atomicMin((unsigned*)(p.level + c), cand);
+                dec = old > cand;
+            }
+            push_vertex(p, dec, c, 0, tag, true, false);
+        }
+        // insertion seeds: thread per half-edit
+        for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
+            int64_t k = b + lane_id();
+            bool dec = false;
+            int32_t y = 0;
+            if (k < nh) {
+                unsigned long long key = p.hkeys[k];
+                int op = (int)((key >> p.B) & 1ull);
+                int32_t x = (int32_t)(key >> (p.B + 1));
+                y = (int32_t)(key & ((1ull << p.B) - 1));
+                if (op == 0) {
+                    int lx = ld_level(p.level + x);
+                    if (lx >= 0) {
+                        unsigned cand = (unsigned)lx + 1;
+                        unsigned old = atomicMin((unsigned*)(p.level + y), cand);
+                        dec = old > cand;
+                    }
+                }
+            }
+            push_vertex(p, dec, y, 0, tag, true, true);
+        }
+        if (!grid_sync(p.bar, 6)) return;
+        cur = 0;
+    }
+    // ---- C: relax rounds -------------------------------------------------------------------
+    while (true) {
+        const int cnt = qcount(p, cur);
+        if (cnt == 0) break;
+        const int nxt = (cur + 1) % 3, zer = (cur + 2) % 3;
+        if (leader) p.ctr->q_count[zer] = 0;
+        tag++;
+        relax_round(p, cur, nxt, tag, bytes);
+        rounds++;
+        if (!grid_sync(p.bar, 7)) return;
+        cur = nxt;
+    }
+    // ---- counters ----------------------------------------------------------------------------
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+    if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
+    if (leader) {
+        p.ctr->rounds = rounds;
+        p.ctr->affected = p.ctr->changed;
+    }
+}
+
+static int bfs_launch(scout_ctx* c, int mode, scout_batch_stats* st) {
+    (void)st;
+    SCOUT_RC(lists_ensure(c));
+    BfsParams p;
+    p.g = dgraph(c);
+    p.level = c->level;
+    p.source = c->source;
+    p.hkeys = c->d_hkeys;
+    p.B = c->key_bits;
+    for (int i = 0; i < 3; i++) p.q[i] = (unsigned long long*)c->d_qbuf[i];
+    p.qcap = c->qcap;
+    p.inval = c->d_list[1];
+    p.touched = c->d_list[0];
+    p.st_inval = c->stamp_a;
+    p.st_touch = c->stamp_b;
+    p.st_q = (uint32_t*)c->stamp_c;
+    p.epoch = (int32_t)c->epoch;
+    p.qtag0 = c->qtag;
+    p.ctr = c->d_ctr;
+    p.bar = c->d_bar;
+    p.mode = mode;
+    void* args[] = {&p};
+    return coop_launch(c, (const void*)k_bfs, BFS_THREADS, args, 0);
+}
+
+int bfs_repair(scout_ctx* c, scout_batch_stats* st) { return bfs_launch(c, 0, st); }
+int bfs_recompute(scout_ctx* c, int32_t source, scout_batch_stats* st) {
+    c->source = source;
+    return bfs_launch(c, 1, st);
+}
+
+}  // namespace scout

@@ -1,0 +1,202 @@
+// ctx.cuh -- the engine context (struct scout_ctx) and host-side helpers shared by the
+// .cu translation units.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "../../../include/scout_gpu.h"
+#include "common.cuh"
+
+// Per-batch device counters, copied back once per batch.
+struct DevCounters {
+    // update phase
+    int n_ins;          // edits classified as insertions
+    int n_del;          // edits classified as deletions
+    int n_half;         // applied half-edits (2 per applied edit)
+    int n_aff;          // vertices whose row changed
+    int n_small, n_large;
+    long long new_elems;      // elements written to the pool this batch
+    long long nnz_delta;      // inserted minus deleted entries
+    long long update_bytes;   // algorithmic bytes of the row merge
+    // repair
+    int q_count[4];           // rotating queue counters
+    int list_count[4];        // auxiliary list counters
+    int rounds;
+    int changed;
+    int affected;
+    int conflicts;
+    int noop;
+    int recomputes;
+    int splits;
+    int searches;
+    int overflow;             // a device list hit its capacity (results invalid)
+    int pad;
+    long long hbm_bytes;      // algorithmic bytes of the repair
+    long long aux64[4];
+};
+
+struct scout_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t s_main = nullptr;
+    cudaStream_t s_copy[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    cudaEvent_t ev_t[6] = {nullptr};
+    uint64_t budget = 0;
+    uint64_t held = 0;
+    std::string err;
+    char name[256] = {0};
+
+    // ---- graph store ----
+    int64_t n = 0;
+    int64_t nnz = 0;           // live entries (host view, exact after each batch)
+    scout::Row* row = nullptr;
+    int32_t* pool = nullptr;
+    int64_t pool_cap = 0;
+    int64_t tail = 0;          // first free pool element (host view)
+    bool reserved = false;
+    bool sealed = false;
+    int32_t* d_tmp_rows = nullptr;   // staging target for rows of one slot
+    int64_t staged_rows = 0;
+
+    // ---- per-problem state ----
+    int32_t* level = nullptr;
+    int32_t* color = nullptr;
+    int32_t* label = nullptr;
+    int32_t* mis = nullptr;
+    int32_t source = 0;
+    int last_problem = -1;
+
+    // ---- persistent per-vertex scratch (stamped with a batch epoch; never cleared) ----
+    int32_t* stamp_a = nullptr;   // e.g. invalid / queued marks
+    int32_t* stamp_b = nullptr;
+    int32_t* stamp_c = nullptr;
+    int32_t* aux_v = nullptr;     // per-vertex int scratch (marker / uf parent)
+    int32_t* aux_w = nullptr;
+    uint32_t epoch = 0;
+
+    // ---- per-batch workspace: one allocation, carved per batch size (grow-only) ----
+    void* ws = nullptr;
+    int64_t ws_bytes = 0;
+    int64_t ws_m = 0;               // edits the workspace is carved for
+    scout_edge* d_edits = nullptr;
+    uint8_t* d_ops = nullptr;
+    uint8_t* d_eflag = nullptr;
+    unsigned long long* d_keys = nullptr;       // half-edit keys (2m)
+    unsigned long long* d_keys_alt = nullptr;   // radix ping-pong (2m)
+    unsigned long long* d_hkeys = nullptr;      // sorted half-edits of the current batch
+    long long* d_mdp = nullptr;     // matched-deletion prefix, aligned with keys (2m)
+    int32_t* d_aff = nullptr;       // affected vertex ids (2m)
+    int64_t* d_aff_seg = nullptr;   // [3 * 2m]: segment begin, first deletion, end
+    int64_t* d_aff_len = nullptr;   // new length, then exclusive offsets (2m + 1)
+    int32_t* d_aff_small = nullptr; // (2m)
+    int32_t* d_aff_large = nullptr; // (2m)
+    int key_bits = 0;
+
+    // ---- per-vertex work lists (n-sized, allocated on first repair) ----
+    void* d_qbuf[3] = {nullptr, nullptr, nullptr};   // queues (uint64 items), qcap each
+    int64_t qcap = 0;
+    int32_t* d_list[2] = {nullptr, nullptr};         // touched / invalid lists, n each
+    int32_t* d_commit = nullptr;                     // (id, value) pairs for the commit (2n)
+    uint32_t qtag = 1;                               // per-round dedupe tags, never reused
+    unsigned int* d_sort_hist = nullptr; int64_t cap_hist = 0;
+    int64_t* d_scan_tmp = nullptr;  int64_t cap_scan = 0;
+    void* d_misc = nullptr;         int64_t cap_misc = 0;   // kernel-specific scratch
+
+    DevCounters* d_ctr = nullptr;
+    DevCounters* h_ctr = nullptr;   // pinned
+    scout::GridBar* d_bar = nullptr;
+    scout::GridBar* h_bar = nullptr; // pinned
+    int* d_flags = nullptr;          // staging / seal error flags (int[16])
+
+    // ---- pinned staging ----
+    void* h_pin_edits = nullptr;  int64_t cap_pin_edits = 0;
+    void* h_pin_commit = nullptr; int64_t cap_pin_commit = 0;
+    void* h_slab[2] = {nullptr, nullptr}; int64_t cap_slab = 0;   // int32 elements
+    int64_t* h_slab_off[2] = {nullptr, nullptr}; int32_t* h_slab_ids[2] = {nullptr, nullptr};
+    int64_t cap_slab_rows = 0;
+    int32_t* d_stage_ids[2] = {nullptr, nullptr};
+    int64_t* d_stage_off[2] = {nullptr, nullptr};
+    int64_t cap_stage_rows = 0;
+
+    // ---- last batch bookkeeping ----
+    int64_t last_changed = 0;
+    int64_t last_half = 0;
+    int64_t last_aff = 0;
+    int32_t coop_blocks = 0;   // resident blocks of the persistent kernels
+
+    int fail(int code, const std::string& msg) { err = msg; return code; }
+};
+
+namespace scout {
+
+// Allocation against the context's HBM budget.
+int dev_alloc(scout_ctx* c, void** p, size_t bytes, const char* what);
+void dev_free(scout_ctx* c, void* p, size_t bytes);
+template <typename T>
+int dev_grow(scout_ctx* c, T** p, int64_t* cap, int64_t need, const char* what) {
+    if (*cap >= need && *p) return SCOUT_OK;
+    int64_t nc = need + need / 4 + 1024;
+    if (*p) dev_free(c, *p, (size_t)*cap * sizeof(T));
+    *p = nullptr;
+    *cap = 0;
+    int rc = dev_alloc(c, (void**)p, (size_t)nc * sizeof(T), what);
+    if (rc != SCOUT_OK) return rc;
+    *cap = nc;
+    return SCOUT_OK;
+}
+int pin_grow(scout_ctx* c, void** p, int64_t* cap_bytes, int64_t need_bytes);
+
+int cuda_fail(scout_ctx* c, cudaError_t e, const char* where);
+#define SCOUT_CU(c, call)                                                  \
+    do {                                                                   \
+        cudaError_t e_ = (call);                                           \
+        if (e_ != cudaSuccess) return ::scout::cuda_fail((c), e_, #call);  \
+    } while (0)
+#define SCOUT_LAUNCH(c, what)                                              \
+    do {                                                                   \
+        cudaError_t e_ = cudaGetLastError();                               \
+        if (e_ != cudaSuccess) return ::scout::cuda_fail((c), e_, what);   \
+    } while (0)
+#define SCOUT_RC(x)                          \
+    do {                                     \
+        int rc_ = (x);                       \
+        if (rc_ != SCOUT_OK) return rc_;     \
+    } while (0)
+
+inline DGraph dgraph(const scout_ctx* c) { return DGraph{c->row, c->pool, (int32_t)c->n}; }
+inline int blocks_for(int64_t items, int threads, int cap = 148 * 32) {
+    int64_t b = (items + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+// sort.cu
+int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, int64_t n, int bits,
+              unsigned long long** sorted_out);
+// scan.cu: exclusive scan of int64 values in place; *total receives the sum (device ptr or null)
+int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total);
+// graph.cu
+int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m, scout_batch_stats* st);
+int graph_ensure_scratch(scout_ctx* c);
+int graph_compact(scout_ctx* c, int64_t min_free);
+int ws_ensure(scout_ctx* c, int64_t m);
+int lists_ensure(scout_ctx* c);
+int batch_begin(scout_ctx* c);   // zeroes the counters and the barrier for a new batch
+int counters_fetch(scout_ctx* c); // copies the device counters into c->h_ctr (synchronous)
+// problem kernels (their .cu files)
+int bfs_repair(scout_ctx* c, scout_batch_stats* st);
+int bfs_recompute(scout_ctx* c, int32_t source, scout_batch_stats* st);
+int cc_repair(scout_ctx* c, const scout_sched* sched, scout_batch_stats* st);
+int cc_recompute(scout_ctx* c, scout_batch_stats* st);
+int coloring_repair(scout_ctx* c, scout_batch_stats* st);
+int mis_repair(scout_ctx* c, scout_batch_stats* st);
+// persistent launch helper
+int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem);
+
+}  // namespace scout

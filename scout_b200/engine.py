@@ -1,0 +1,364 @@
+"""Python face of libscout.so: numpy in, numpy out.
+
+    ctx = Context(device=0)
+    ctx.load_csr(off, adj)                  # graph resident in HBM
+    ctx.upload("bfs", levels)               # maintained solution
+    stats = ctx.repair("bfs", edges)        # one batch of toggles (N x 2 int32, 0-indexed)
+    changed = ctx.commit("bfs", mirror)     # changed entries copied into a host mirror
+
+Host-only helpers (no GPU): R-MAT generation, update streams, initial states, .egr and
+text-format I/O, and the storage-resident hybrid graph.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import LIB, PROBLEMS, ScoutBatchStats, ScoutEdge, ScoutSched
+
+
+class ScoutError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_lib.ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _check(rc: int, ctx=None) -> None:
+    if rc != _lib.SCOUT_OK:
+        msg = LIB.scout_last_error(ctx)
+        raise ScoutError(rc, msg.decode() if msg else "")
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _i64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _pedge(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(ScoutEdge))
+
+
+def _prob(p) -> int:
+    return PROBLEMS[p] if isinstance(p, str) else int(p)
+
+
+def as_edges(e) -> np.ndarray:
+    a = _i32(e)
+    if a.ndim != 2 or a.shape[1] != 2:
+        raise ValueError("edges must have shape (m, 2)")
+    return a
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    _check(LIB.scout_device_count(C.byref(n)))
+    return n.value
+
+
+class Context:
+    """One device context: an HBM graph store plus the maintained solutions."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        h = C.c_void_p()
+        _check(LIB.scout_ctx_create(int(device), int(budget_bytes), C.byref(h)))
+        self._h = h
+        self.n = 0
+
+    def close(self) -> None:
+        if self._h:
+            LIB.scout_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc: int) -> None:
+        _check(rc, self._h)
+
+    # ---- graph ------------------------------------------------------------------------
+    def load_csr(self, off, adj) -> None:
+        off = _i64(off)
+        adj = _i32(adj)
+        n = len(off) - 1
+        self._c(LIB.scout_graph_load_csr(self._h, n, _p64(off), _p32(adj)))
+        self.n = n
+
+    def reserve(self, n: int, nnz: int) -> None:
+        self._c(LIB.scout_graph_reserve(self._h, int(n), int(nnz)))
+        self.n = int(n)
+
+    def stage_rows(self, slot: int, ids, offs, elems) -> None:
+        ids, offs, elems = _i32(ids), _i64(offs), _i32(elems)
+        self._c(LIB.scout_stage_rows(self._h, int(slot), _p32(ids), _p64(offs), _p32(elems), len(ids),
+                                     int(offs[-1] - offs[0]) if len(offs) else 0))
+
+    def seal(self) -> None:
+        self._c(LIB.scout_graph_seal(self._h))
+
+    def info(self) -> dict:
+        v = [C.c_int64() for _ in range(4)]
+        self._c(LIB.scout_graph_info(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("n", "nnz", "pool_used", "pool_cap"), (x.value for x in v)))
+
+    def graph(self):
+        """Current adjacency as CSR (rows ascending)."""
+        n = self.info()["n"]
+        off = np.zeros(n + 1, dtype=np.int64)
+        rc = LIB.scout_graph_download(self._h, _p64(off), None, 0)
+        if rc not in (_lib.SCOUT_OK, -3):
+            self._c(rc)
+        adj = np.zeros(max(int(off[n]), 1), dtype=np.int32)
+        self._c(LIB.scout_graph_download(self._h, _p64(off), _p32(adj), len(adj)))
+        return off, adj[: int(off[n])]
+
+    def compact(self) -> None:
+        self._c(LIB.scout_graph_compact(self._h))
+
+    def classify(self, edges) -> np.ndarray:
+        e = as_edges(edges)
+        out = np.zeros(len(e), dtype=np.uint8)
+        self._c(LIB.scout_classify(self._h, _pedge(e), len(e), out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out
+
+    # ---- state ------------------------------------------------------------------------
+    def upload(self, problem, sol) -> None:
+        s = _i32(sol)
+        self._c(LIB.scout_state_upload(self._h, _prob(problem), _p32(s), len(s)))
+
+    def download(self, problem) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int32)
+        self._c(LIB.scout_state_download(self._h, _prob(problem), _p32(out), self.n))
+        return out
+
+    def set_source(self, s: int) -> None:
+        self._c(LIB.scout_set_source(self._h, int(s)))
+
+    # ---- repair -----------------------------------------------------------------------
+    def repair(self, problem, edges, ops=None, sched: Optional[dict] = None) -> dict:
+        e = as_edges(edges)
+        st = ScoutBatchStats()
+        sd = ScoutSched()
+        for k, v in (sched or {}).items():
+            setattr(sd, k, v)
+        op = None
+        if ops is not None:
+            ops = np.ascontiguousarray(ops, dtype=np.uint8)
+            op = ops.ctypes.data_as(C.POINTER(C.c_uint8))
+        self._c(LIB.scout_repair(self._h, _prob(problem), _pedge(e), op, len(e), C.byref(sd), C.byref(st)))
+        return st.as_dict()
+
+    def commit(self, problem, mirror: np.ndarray) -> int:
+        if mirror.dtype != np.int32 or not mirror.flags.c_contiguous:
+            raise ValueError("mirror must be a contiguous int32 array")
+        ch = C.c_int64()
+        self._c(LIB.scout_commit(self._h, _prob(problem), _p32(mirror), len(mirror), C.byref(ch)))
+        return ch.value
+
+    def recompute_bfs(self, source: int = 0) -> dict:
+        st = ScoutBatchStats()
+        self._c(LIB.scout_recompute_bfs(self._h, int(source), C.byref(st)))
+        return st.as_dict()
+
+    def recompute_cc(self) -> dict:
+        st = ScoutBatchStats()
+        self._c(LIB.scout_recompute_cc(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def sync(self, timeout_us: int = 0) -> None:
+        self._c(LIB.scout_sync(self._h, int(timeout_us)))
+
+
+# ---------------------------------------------------------------------------------------
+# Host-only helpers
+# ---------------------------------------------------------------------------------------
+class HostCsr:
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_arrays(cls, off, adj) -> "HostCsr":
+        off, adj = _i64(off), _i32(adj)
+        h = C.c_void_p()
+        _check(LIB.scout_csr_from_arrays(len(off) - 1, _p64(off), _p32(adj), C.byref(h)))
+        return cls(h)
+
+    @property
+    def n(self) -> int:
+        return LIB.scout_csr_nodes(self._h)
+
+    @property
+    def nnz(self) -> int:
+        return LIB.scout_csr_nnz(self._h)
+
+    def arrays(self):
+        n, nnz = self.n, self.nnz
+        off = np.ctypeslib.as_array(LIB.scout_csr_offsets(self._h), shape=(n + 1,)).copy()
+        adj = np.ctypeslib.as_array(LIB.scout_csr_adj(self._h), shape=(max(nnz, 1),))[:nnz].copy()
+        return off, adj
+
+    def stream(self, kind: int, batch_size: int, nbatches: int, insert_ratio: float = 0.5,
+               lowdeg_frac: float = 0.0, seed: int = 1) -> np.ndarray:
+        out = np.zeros((batch_size * nbatches, 2), dtype=np.int32)
+        _check(LIB.scout_gen_stream(self._h, int(kind), int(batch_size), int(nbatches), float(insert_ratio),
+                                    float(lowdeg_frac), int(seed), _pedge(out)))
+        return out
+
+    def init_state(self, problem, source: int = 0) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int32)
+        _check(LIB.scout_init_state(self._h, _prob(problem), int(source), _p32(out)))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            LIB.scout_csr_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1) -> HostCsr:
+    h = C.c_void_p()
+    _check(LIB.scout_gen_rmat(int(scale), int(edge_factor), a, b, c, int(seed), C.byref(h)))
+    return HostCsr(h)
+
+
+def read_egr(path: str):
+    h = C.c_void_p()
+    _check(LIB.scout_egr_open(path.encode(), 1, C.byref(h)))
+    try:
+        n = LIB.scout_egr_nodes(h)
+        e = LIB.scout_egr_edges(h)
+        off = np.zeros(n + 1, dtype=np.int64)
+        _check(LIB.scout_egr_offsets(h, _p64(off)))
+        adj = np.ctypeslib.as_array(LIB.scout_egr_nlist(h), shape=(max(e, 1),))[:e].copy() if e else np.zeros(0, np.int32)
+        wide = bool(LIB.scout_egr_is_wide(h))
+    finally:
+        LIB.scout_egr_close(h)
+    return off, adj, wide
+
+
+def write_egr(path: str, off, adj, wide: bool = False) -> None:
+    off, adj = _i64(off), _i32(adj)
+    _check(LIB.scout_egr_write(path.encode(), len(off) - 1, _p64(off), _p32(adj), int(wide)))
+
+
+def parse_batch_file(path: str, n: int) -> np.ndarray:
+    m = C.c_int64()
+    rc = LIB.scout_parse_batch_file(path.encode(), int(n), None, 0, C.byref(m))
+    if rc not in (_lib.SCOUT_OK, -3):
+        _check(rc)
+    out = np.zeros((max(m.value, 1), 2), dtype=np.int32)
+    _check(LIB.scout_parse_batch_file(path.encode(), int(n), _pedge(out), len(out), C.byref(m)))
+    return out[: m.value]
+
+
+def read_ints(path: str) -> np.ndarray:
+    m = C.c_int64()
+    rc = LIB.scout_read_ints(path.encode(), None, 0, C.byref(m))
+    if rc not in (_lib.SCOUT_OK, -3):
+        _check(rc)
+    out = np.zeros(max(m.value, 1), dtype=np.int64)
+    _check(LIB.scout_read_ints(path.encode(), _p64(out), len(out), C.byref(m)))
+    return out[: m.value]
+
+
+def load_state(path: str, problem, n: int):
+    sol = np.zeros(n, dtype=np.int32)
+    aux = C.c_int64()
+    _check(LIB.scout_load_state(path.encode(), _prob(problem), int(n), _p32(sol), C.byref(aux)))
+    return sol, aux.value
+
+
+def write_state(path: str, problem, sol) -> None:
+    s = _i32(sol)
+    _check(LIB.scout_write_state(path.encode(), _prob(problem), len(s), _p32(s)))
+
+
+def write_batch_folder(path: str, edges, batch_size: int, nbatches: int) -> None:
+    e = as_edges(edges)
+    if len(e) < batch_size * nbatches:
+        raise ValueError("not enough edges for the requested batches")
+    _check(LIB.scout_write_batch_folder(path.encode(), _pedge(e), int(batch_size), int(nbatches)))
+
+
+class HybridGraph:
+    """Storage-resident .egr (mmap) + edge-update scratchpad (host)."""
+
+    def __init__(self, path: str, madv_random: bool = True):
+        h = C.c_void_p()
+        _check(LIB.scout_hgraph_open(path.encode(), int(madv_random), C.byref(h)))
+        self._h = h
+
+    @property
+    def n(self) -> int:
+        return LIB.scout_hgraph_nodes(self._h)
+
+    def is_adjacent(self, u: int, v: int) -> bool:
+        r = LIB.scout_hgraph_is_adjacent(self._h, u, v)
+        if r < 0:
+            _check(r)
+        return bool(r)
+
+    def insert(self, u: int, v: int) -> None:
+        _check(LIB.scout_hgraph_insert(self._h, u, v))
+
+    def remove(self, u: int, v: int) -> None:
+        _check(LIB.scout_hgraph_remove(self._h, u, v))
+
+    def degree(self, v: int) -> int:
+        d = LIB.scout_hgraph_degree(self._h, v)
+        if d < 0:
+            _check(int(d))
+        return d
+
+    def neighbors(self, v: int) -> np.ndarray:
+        d = self.degree(v)
+        out = np.zeros(max(d, 1), dtype=np.int32)
+        LIB.scout_hgraph_neighbors(self._h, v, _p32(out), len(out))
+        return out[:d]
+
+    def compact(self, out_path: str) -> None:
+        _check(LIB.scout_hgraph_compact(self._h, out_path.encode()))
+
+    def fetch_all(self, ctx: Context, slab_elems: int = 0) -> None:
+        _check(LIB.scout_fetch_all(self._h, ctx._h, int(slab_elems)), ctx._h)
+        ctx.n = self.n
+
+    def close(self) -> None:
+        if self._h:
+            LIB.scout_hgraph_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
