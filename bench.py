@@ -1,0 +1,405 @@
+#!/usr/bin/env python3
+"""Edge-updates/s of the B200 dynamic-graph repair engine.
+
+Workload (one step = one batch of toggled edges through the hot path): an R-MAT graph of
+scale 22 (4,194,304 vertices, edge factor 16, a/b/c/d = .57/.19/.19/.05, symmetrised, no
+self-loops or duplicates, ~128M directed entries, 0.5 GB of adjacency: larger than the 126 MB
+L2), initial BFS levels from vertex 0 and a greedy smallest-free colouring; batches of
+10^4, 10^5 and 10^6 toggles whose endpoints are drawn proportional to degree, half
+deletions of existing edges and half insertions of non-edges. Seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl scout|reference]
+
+value  edge-updates/s with the edits already in HBM: classification + merge into the rows +
+       repair, from the library's CUDA events on its own stream.
+e2e    the same through the public C ABI with host buffers: each step copies the edits from
+       host memory, repairs and copies the changed solution entries back into a host mirror
+       (scout_repair + scout_commit), timed with CUDA events around the step loop.
+Multi-GPU (torchrun): every rank runs an independent replica stream (no collective on the
+data path), value = all ranks' updates / max over ranks of the elapsed time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZES = (10_000, 100_000, 1_000_000)
+METRIC = "edge-updates/sec per problem"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="scout", choices=["scout", "reference"])
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--problems", default="bfs")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-sample", type=int, default=20000, help="edits per batch timed in the reference arm")
+    ap.add_argument("--ref-timeout", type=float, default=150.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", 0))
+        self.world = int(os.environ.get("WORLD_SIZE", 1))
+        self.local = int(os.environ.get("LOCAL_RANK", 0))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device=f"cuda:{self.local}")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize(self.local)
+
+    def reduce(self, x: float, op: str) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX if op == "max" else self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------------------
+def batch_sizes(steps: int, warmup: int):
+    return [SIZES[i % len(SIZES)] for i in range(warmup + steps)]
+
+
+def make_workload(scale: int, seed: int, stream_seed: int, sizes):
+    import scout_b200 as sb
+    g = sb.gen_rmat(scale, 16, seed=seed)
+    off, adj = g.arrays()
+    total = sum(sizes)
+    s = g.stream(sb.STREAM_PREFERENTIAL, total, 1, insert_ratio=0.5, seed=stream_seed)
+    bounds = np.cumsum([0] + list(sizes))
+    batches = [np.ascontiguousarray(s[bounds[i]:bounds[i + 1]]) for i in range(len(sizes))]
+    init = {"bfs": g.init_state("bfs", 0), "coloring": g.init_state("coloring"), "cc": g.init_state("cc"),
+            "mis": g.init_state("mis")}
+    return g, off, adj, batches, init
+
+
+class Clocks:
+    """SM clock and throttle-reason sampling during the timed loops only.
+
+    The timed region lasts tens of milliseconds, shorter than nvidia-smi's 200 ms loop, so the
+    clocks are polled through NVML every 5 ms from a thread while a timed loop runs (the same
+    counters nvidia-smi reports: clocks.sm, clocks.max.sm, clocks_event_reasons.*)."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self.reasons = 0
+        self._stop = threading.Event()
+        self._t = None
+        self.h = None
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(gpu)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.h = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)))
+                self.reasons |= int(self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                pass
+            self._stop.wait(0.005)
+
+    def start(self):
+        if self.h is not None:
+            self._stop.clear()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+
+    def stop(self):
+        if self._t:
+            self._stop.set()
+            self._t.join()
+            self._t = None
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "sm_mhz_min": min(self.samples), "sm_mhz_max": max(self.samples),
+                "reasons": sorted(k for k, bit in self.REASONS.items() if self.reasons & bit),
+                "samples": len(self.samples), "source": "NVML, 5 ms polling inside the timed loops"}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------
+# scout arm
+# ---------------------------------------------------------------------------------------
+def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, clocks):
+    import torch
+
+    import scout_b200 as sb
+    ctx = sb.Context(device)
+    ctx.load_csr(off, adj)
+    ctx.upload(problem, init)
+    mirror = init.copy()
+    for b in batches[:warmup]:
+        ctx.repair(problem, b)
+        ctx.commit(problem, mirror)
+    timed = batches[warmup:warmup + steps]
+    per = []
+    torch.cuda.set_device(device)
+    dist.barrier()
+    torch.cuda.synchronize(device)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.start()
+    ev0.record()
+    for b in timed:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = ctx.repair(problem, b)
+        changed = ctx.commit(problem, mirror)
+        e1.record()
+        st["commit_changed"] = changed
+        st["_ev"] = (e0, e1)
+        per.append(st)
+    ev1.record()
+    torch.cuda.synchronize(device)
+    clocks.stop()
+    dist.barrier()
+    e2e_ms = ev0.elapsed_time(ev1)
+    for st in per:
+        e0, e1 = st.pop("_ev")
+        st["ms_step"] = e0.elapsed_time(e1)
+    ctx.close()
+    return per, e2e_ms
+
+
+def cpu_baseline(problem, off, adj, init, batches, seconds):
+    """The oracle (single-thread CPU restatement of the reference engine) on a bounded sample."""
+    from oracle import oracle as orc
+    eng = orc.Engine(problem, off, adj, init)
+    edits = 0
+    t_used = 0.0
+    k = 0
+    for b in batches:
+        if t_used >= seconds:
+            break
+        t0 = time.perf_counter()
+        eng.batch(b)
+        t_used += time.perf_counter() - t0
+        edits += len(b)
+        k += 1
+    return {"value": edits / t_used if t_used else None, "unit": "edge-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{problem}: first {k} batches ({edits} toggles) of the same stream, oracle restatement "
+                      f"of the reference engine, {t_used:.1f} s single-threaded"}
+
+
+def scout_arm(a, dist):
+    import scout_b200 as sb
+    sizes = batch_sizes(a.steps, a.warmup)
+    g, off, adj, batches, init = make_workload(a.scale, a.seed, 1000 + a.seed + dist.rank, sizes)
+    problems = [p.strip() for p in a.problems.split(",") if p.strip()]
+    device = dist.local
+    results = {}
+    clocks = Clocks(device)
+    for p in problems:
+        results[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks)
+    clk = clocks.summary()
+    peak, peak_kind = measured_peak()
+    per_problem = {}
+    tot_edits = tot_e2e = tot_dev = 0.0
+    all_ms = []
+    bytes_rep = bytes_upd = ms_rep = ms_upd = 0.0
+    launches = h2d = d2h = 0
+    for p, (per, e2e_ms) in results.items():
+        edits = sum(s["edits"] for s in per)
+        dev_ms = sum(s["ms_update"] + s["ms_repair"] for s in per)
+        per_problem[p] = {"edge_updates_per_s": edits / (dev_ms / 1e3), "e2e_edge_updates_per_s": edits / (e2e_ms / 1e3),
+                          "p50_batch_ms": float(np.percentile([s["ms_step"] for s in per], 50)),
+                          "p99_batch_ms": float(np.percentile([s["ms_step"] for s in per], 99)),
+                          "batches": len(per), "edits": edits,
+                          "repair_ms": sum(s["ms_repair"] for s in per), "update_ms": sum(s["ms_update"] for s in per),
+                          "h2d_ms": sum(s["ms_h2d"] for s in per), "rounds": sum(s["rounds"] for s in per),
+                          "changed": sum(s["commit_changed"] for s in per)}
+        tot_edits += edits
+        tot_e2e += e2e_ms
+        tot_dev += dev_ms
+        all_ms += [s["ms_step"] for s in per]
+        bytes_rep += sum(s["hbm_bytes"] for s in per)
+        bytes_upd += sum(s["update_bytes"] for s in per)
+        ms_rep += sum(s["ms_repair"] for s in per)
+        ms_upd += sum(s["ms_update"] for s in per)
+        launches += sum(s["launches"] for s in per)
+        h2d += sum(s["h2d_bytes"] for s in per)
+        d2h += sum(s["d2h_bytes"] + 8 * s["commit_changed"] for s in per)
+    n_steps = sum(len(r[0]) for r in results.values())
+    # whole job over ranks
+    edits_all = dist.reduce(tot_edits, "sum")
+    dev_s = dist.reduce(tot_dev / 1e3, "max")
+    e2e_s = dist.reduce(tot_e2e / 1e3, "max")
+    # roofline of the dominant kernel (repair vs merge), algorithmic bytes / event time
+    if ms_rep >= ms_upd:
+        kern, b, ms = "repair (k_bfs / problem kernel)", bytes_rep, ms_rep
+    else:
+        kern, b, ms = "batch merge (k_classify..k_merge)", bytes_upd, ms_upd
+    achieved = b / (ms / 1e3) / 1e9 if ms else 0.0
+    line = {
+        "metric": METRIC, "value": edits_all / dev_s if dev_s else None, "unit": "edge-updates/s",
+        "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * e2e_s / max(n_steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT + preferential toggle stream)",
+        "config": {"workload": f"R-MAT scale {a.scale} EF16 (.57/.19/.19/.05) seed {a.seed}; "
+                               f"preferential 50/50 toggles; batch sizes {list(SIZES)} cycled; problems {problems}",
+                   "vertices": int(g.n), "directed_entries": int(g.nnz), "graph_bytes": int(4 * g.nnz + 8 * g.n),
+                   "l2": "inputs larger than L2 (0.5 GB adjacency vs 126 MB L2); no flush",
+                   "parallelism": f"replicas x{dist.world}", "batch_sizes": sizes[a.warmup:]},
+        "p50_batch_ms": float(np.percentile(all_ms, 50)), "p99_batch_ms": float(np.percentile(all_ms, 99)),
+        "per_problem": per_problem,
+        "e2e": {"value": edits_all / e2e_s if e2e_s else None, "unit": "edge-updates/s",
+                "h2d_bytes_per_step": int(h2d / max(n_steps, 1)), "d2h_bytes_per_step": int(d2h / max(n_steps, 1))},
+        "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": b / max(n_steps, 1)},
+        "roofline_merge": {"achieved": bytes_upd / (ms_upd / 1e3) / 1e9 if ms_upd else 0.0,
+                           "ms": ms_upd, "bytes": bytes_upd},
+        "roofline_repair": {"achieved": bytes_rep / (ms_rep / 1e3) / 1e9 if ms_rep else 0.0,
+                            "ms": ms_rep, "bytes": bytes_rep},
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
+        p0 = problems[0]
+        line["cpu_baseline"] = cpu_baseline(p0, off, adj, init[p0], batches, a.cpu_seconds)
+    return line
+
+
+# ---------------------------------------------------------------------------------------
+# reference arm: the reference's own programs (oracle/_ref, compiled from its sources)
+# ---------------------------------------------------------------------------------------
+BATCH_RE = re.compile(r"^Batch (\d+)/(\d+) \| edges=(\d+) \| time=([0-9.]+)ms")
+
+
+def reference_arm(a, dist):
+    import scout_b200 as sb
+    sizes = batch_sizes(a.steps, a.warmup)
+    problems = [p.strip() for p in a.problems.split(",") if p.strip()]
+    g, off, adj, batches, init = make_workload(a.scale, a.seed, 1000 + a.seed, sizes)
+    sample = [b[: a.ref_sample] for b in batches]
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    have = all(os.path.exists(os.path.join(ref_dir, f"scout_{p}")) for p in problems)
+    cores = os.cpu_count()
+    if not have:
+        # the oracle port of the reference engine on the host cores (single thread)
+        cb = cpu_baseline(problems[0], off, adj, init[problems[0]], sample, a.cpu_seconds * 2)
+        return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "edge-updates/s",
+                "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0}}
+    per_problem = {}
+    edits_t = ms_t = 0.0
+    with tempfile.TemporaryDirectory() as td:
+        egr = os.path.join(td, "g.egr")
+        sb.write_egr(egr, off, adj, wide=False)
+        bdir = os.path.join(td, "batches")
+        os.makedirs(bdir)
+        for k, b in enumerate(sample):
+            sb.write_batch_folder(os.path.join(td, "one"), b, len(b), 1)
+            os.replace(os.path.join(td, "one", "1.mtx"), os.path.join(bdir, f"{k + 1}.mtx"))
+        for p in problems:
+            st = os.path.join(td, f"{p}.txt")
+            sb.write_state(st, p, init[p])
+            cmd = [os.path.join(ref_dir, f"scout_{p}"), egr, st, bdir, str(len(sample)), str(dist.local)]
+            env = dict(os.environ, SCOUT_SKIP_COMPACTION="1")
+            try:
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=a.ref_timeout, env=env, cwd=td)
+                out = r.stdout
+            except subprocess.TimeoutExpired as e:
+                out = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
+            rows = [BATCH_RE.match(l) for l in out.splitlines()]
+            rows = [(int(m.group(1)), int(m.group(3)), float(m.group(4))) for m in rows if m]
+            timed = [r for r in rows if r[0] > a.warmup]
+            e = sum(r[1] for r in timed)
+            ms = sum(r[2] for r in timed)
+            per_problem[p] = {"edge_updates_per_s": e / (ms / 1e3) if ms else None, "batches_timed": len(timed),
+                              "edits": e, "ms": ms}
+            edits_t += e
+            ms_t += ms
+    val = edits_t / (ms_t / 1e3) if ms_t else None
+    return {"impl": "reference", "metric": METRIC, "value": val, "unit": "edge-updates/s", "n_gpus": dist.world,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "dtype": "int32",
+            "data": "synthetic (seeded R-MAT + preferential toggle stream)",
+            "config": {"workload": f"R-MAT scale {a.scale} EF16 seed {a.seed}; preferential 50/50 toggles; "
+                                   f"first {a.ref_sample} toggles of each batch; problems {problems}"},
+            "per_problem": per_problem,
+            "cpu_baseline": {"value": val, "unit": "edge-updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"reference binaries (src/*/scout_*.cu built for sm_100a, OpenMP host "
+                                       f"fetch) on the first {a.ref_sample} toggles of each batch; their own "
+                                       f"per-batch time= lines, warm-up batches excluded"},
+            "e2e": {"value": val, "unit": "edge-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse_args()
+    dist = Dist()
+    try:
+        if a.impl == "reference":
+            if dist.rank != 0:
+                return
+            line = reference_arm(a, dist)
+        else:
+            line = scout_arm(a, dist)
+        if dist.rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

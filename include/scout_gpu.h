@@ -84,12 +84,15 @@ typedef struct scout_batch_stats {
     int64_t hbm_bytes;    /* algorithmic HBM bytes of the repair kernels              */
     int64_t h2d_bytes;    /* host-to-device bytes of the call                         */
     int64_t d2h_bytes;    /* device-to-host bytes of the call                         */
-    double  ms_update;    /* device: classification + merge of the edits into HBM rows */
+    double  ms_update;    /* device: classification + merge of the edits into HBM rows
+                             (edits already in HBM)                                  */
     double  ms_repair;    /* device: repair kernels                                  */
     double  ms_commit;    /* device: changed-entry gather + copy back                */
     double  ms_total;     /* host wall time of the call                              */
     int64_t update_bytes; /* algorithmic HBM bytes of the row merge                   */
-    int64_t reserved[7];
+    int64_t launches;     /* kernels launched by the call                             */
+    double  ms_h2d;       /* device: copy of the edits into HBM                       */
+    int64_t reserved[5];
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;

@@ -37,7 +37,8 @@ class ScoutBatchStats(C.Structure):
                 ("splits", C.c_int64), ("searches", C.c_int64), ("hbm_bytes", C.c_int64),
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("ms_update", C.c_double),
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
-                ("update_bytes", C.c_int64), ("reserved", C.c_int64 * 7)]
+                ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
+                ("reserved", C.c_int64 * 5)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}

@@ -60,6 +60,7 @@ int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t s
     per_sm = std::min(per_sm, 4);
     dim3 grid((unsigned)(per_sm * c->sm_count)), block((unsigned)threads);
     SCOUT_CU(c, cudaLaunchCooperativeKernel(fn, grid, block, args, smem, c->s_main));
+    c->nlaunch += 1;
     return SCOUT_OK;
 }
 
@@ -68,7 +69,7 @@ static void release(scout_ctx* c) {
     cudaSetDevice(c->device);
     if (c->s_main) cudaStreamSynchronize(c->s_main);
     for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
-    void* devs[] = {c->row, c->pool, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c,
+    void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
                     c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_misc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
                     c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
@@ -252,6 +253,7 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     std::memset(&sd, 0, sizeof(sd));
     if (sched) sd = *sched;
     c->last_problem = problem;
+    const int64_t launch0 = c->nlaunch;
     SCOUT_RC(batch_begin(c));
     SCOUT_RC(lists_ensure(c));
     c->epoch++;
@@ -286,7 +288,9 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     st->hbm_bytes = h.hbm_bytes;
     st->update_bytes = h.update_bytes;
     st->d2h_bytes += sizeof(DevCounters);
-    st->ms_update = ev_ms(c->ev_t[0], c->ev_t[1]);
+    st->ms_h2d = ev_ms(c->ev_t[0], c->ev_t[3]);
+    st->ms_update = ev_ms(c->ev_t[3], c->ev_t[1]);
+    st->launches = c->nlaunch - launch0;
     st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
     c->last_changed = h.changed;
     st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -310,6 +314,7 @@ int scout_commit(scout_ctx* c, int problem, int32_t* mirror, int64_t n, int64_t*
         SCOUT_RC(pin_grow(c, &c->h_pin_commit, &c->cap_pin_commit, cnt * 8));
         k_commit_gather<<<blocks_for(cnt, 256), 256, 0, c->s_main>>>(c->d_list[0], c->d_ctr, *slot, c->d_commit);
         SCOUT_LAUNCH(c, "k_commit_gather");
+        c->nlaunch += 1;
         SCOUT_CU(c, cudaMemcpyAsync(c->h_pin_commit, c->d_commit, (size_t)cnt * 8, cudaMemcpyDeviceToHost, c->s_main));
         SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
         const int32_t* p = (const int32_t*)c->h_pin_commit;

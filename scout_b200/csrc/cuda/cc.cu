@@ -1,0 +1,487 @@
+// cc.cu -- exact batch-dynamic connected components with min-vertex-id labels.
+//
+// Replaces the reference's host-only processBatch (scout_cc.cu:392-441): insertions unite
+// labels (lower wins, 365-370); each deletion runs a bidirectional search from both endpoints
+// that always expands the smaller frontier and gives up past a bound (300-342; bound 5000, or
+// unbounded below average degree 10, 469); unresolved deletions wait for one recompute after
+// the stream (516-527). Here every batch ends with the exact partition:
+//   P0  inserted edges hook label roots in a union-find over labels (lower root wins), then
+//       every vertex takes its root, which is the minimum vertex id of the merged class
+//   P1  each deletion gets one block: common-neighbour check, then the bounded bidirectional
+//       search in shared-memory hash sets (the reference's rule, expanded in parallel);
+//       outcomes: connected, split (the exhausted side is a whole component), inconclusive
+//   P2  a class with exactly one split and no inconclusive search splits in two: the side gets
+//       its minimum id as label; when the side holds the class minimum, the remainder gets
+//       its own minimum. A class with more outcomes is marked dirty
+//   P3  dirty classes are recomputed exactly: CAS union-find (lower root wins) over the rows
+//       of their vertices, then label = root
+// A full recompute (scout_recompute_cc) is P3 with every class dirty. One cooperative launch,
+// phases separated by the bounded grid barrier.
+#include "ctx.cuh"
+
+namespace scout {
+
+constexpr int CC_THREADS = 256;
+constexpr int CC_HCAP = 8192;     // shared hash-set slots per side
+constexpr int CC_FCAP = 4096;     // frontier capacity
+constexpr int CC_MAX_BOUND = 4000;
+constexpr int CC_BIG = 4096;      // rows longer than this are scanned by a whole block in P3
+constexpr size_t CC_SMEM = (size_t)(2 * CC_HCAP + 3 * CC_FCAP) * sizeof(int32_t);
+
+struct CcParams {
+    DGraph g;
+    int32_t* label;
+    const unsigned long long* hkeys;
+    int B;
+    int32_t* uf;        // union-find over labels (identity at rest)
+    int32_t* cnt;       // splits per class (zero at rest)
+    int32_t* dirty;     // == epoch: class recomputed this batch
+    int32_t* remf;      // == epoch: class remainder needs its new minimum
+    int32_t* newmin;    // remainder minimum per class (INT32_MAX at rest)
+    int32_t* vp;        // vertex union-find for recomputes
+    int32_t* merged;    // labels hooked this batch (n)
+    unsigned long long* rec;   // split records: (class << 32 | min), (offset << 32 | size)
+    int64_t rec_cap;
+    int32_t* side;      // split vertex buffer
+    int64_t side_cap;
+    int32_t* touched;
+    int32_t* st_touch;
+    int32_t* st_side;   // == epoch: vertex is in a split side this batch
+    int32_t epoch;
+    int bound;
+    int full;           // 1: recompute every class
+    DevCounters* ctr;
+    GridBar* bar;
+};
+
+__device__ __forceinline__ int32_t uf_find(int32_t* uf, int32_t x) {
+    int32_t p = ld_volatile(uf + x);
+    while (p != x) {
+        int32_t gp = ld_volatile(uf + p);
+        if (gp != p) atomicCAS(uf + x, p, gp);   // path halving
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+// Lower root wins; returns the root that was hooked (or -1 when already joined).
+__device__ __forceinline__ int32_t uf_union(int32_t* uf, int32_t a, int32_t b) {
+    while (true) {
+        a = uf_find(uf, a);
+        b = uf_find(uf, b);
+        if (a == b) return -1;
+        int32_t hi = a > b ? a : b, lo = a > b ? b : a;
+        if (atomicCAS(uf + hi, hi, lo) == hi) return hi;
+    }
+}
+
+__device__ __forceinline__ void cc_touch(const CcParams& p, bool pred, int32_t v) {
+    bool nt = false;
+    if (pred) nt = atomicExch(&p.st_touch[v], p.epoch) != p.epoch;
+    int at = warp_append(nt, &p.ctr->changed);
+    if (nt) p.touched[at] = v;
+}
+
+// ---- shared-memory hash set (open addressing, -1 empty) ------------------------------------
+__device__ __forceinline__ unsigned hslot(int32_t x) { return ((unsigned)x * 2654435761u) & (CC_HCAP - 1); }
+__device__ __forceinline__ bool hs_has(const int32_t* hs, int32_t x) {
+    unsigned h = hslot(x);
+    for (int i = 0; i < CC_HCAP; i++) {
+        int32_t s = hs[h];
+        if (s == x) return true;
+        if (s == -1) return false;
+        h = (h + 1) & (CC_HCAP - 1);
+    }
+    return false;
+}
+// 1 inserted, 0 present, -1 full
+__device__ __forceinline__ int hs_insert(int32_t* hs, int32_t x) {
+    unsigned h = hslot(x);
+    for (int i = 0; i < CC_HCAP; i++) {
+        int32_t prev = atomicCAS(hs + h, -1, x);
+        if (prev == -1) return 1;
+        if (prev == x) return 0;
+        h = (h + 1) & (CC_HCAP - 1);
+    }
+    return -1;
+}
+
+// Bounded bidirectional search of one deletion (u, v) by the whole block.
+// Returns 0 connected, 1 split (side written to p.side), 2 inconclusive.
+__device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, long long& bytes) {
+    extern __shared__ int32_t sm[];
+    int32_t* hs[2] = {sm, sm + CC_HCAP};
+    int32_t* fr[2] = {sm + 2 * CC_HCAP, sm + 2 * CC_HCAP + CC_FCAP};
+    int32_t* nf = sm + 2 * CC_HCAP + 2 * CC_FCAP;
+    __shared__ int s_fn[2], s_nn, s_touched, s_met, s_over;
+    const int t = threadIdx.x;
+    // common-neighbour check: both endpoints adjacent to some w (settles hub-hub deletions)
+    if (t == 0) s_met = 0;
+    __syncthreads();
+    {
+        Row ru = p.g.row[u], rv = p.g.row[v];
+        if (rv.len < ru.len) { Row tmp = ru; ru = rv; rv = tmp; }
+        const int32_t* a = p.g.pool + ru.start;
+        const int32_t* b = p.g.pool + rv.start;
+        for (int i = t; i < ru.len && !ld_volatile(&s_met); i += CC_THREADS) {
+            long long k = lower_bound_i32(b, rv.len, a[i]);
+            if (k < rv.len && b[k] == a[i]) s_met = 1;
+        }
+        bytes += 4LL * ((ru.len + CC_THREADS - 1 - t) / CC_THREADS) * 8;
+    }
+    __syncthreads();
+    if (s_met) return 0;
+    for (int i = t; i < 2 * CC_HCAP; i += CC_THREADS) sm[i] = -1;
+    __syncthreads();
+    if (t == 0) {
+        hs_insert(hs[0], u);
+        hs_insert(hs[1], v);
+        fr[0][0] = u;
+        fr[1][0] = v;
+        s_fn[0] = 1;
+        s_fn[1] = 1;
+        s_touched = 2;
+        s_met = 0;
+        s_over = 0;
+    }
+    __syncthreads();
+    while (s_fn[0] > 0 && s_fn[1] > 0) {
+        const int sd = s_fn[0] <= s_fn[1] ? 0 : 1;   // expand the smaller frontier
+        const int fn = s_fn[sd];
+        if (t == 0) s_nn = 0;
+        __syncthreads();
+        // warp per frontier vertex, lanes over its row
+        for (int i = t / WARP; i < fn; i += CC_THREADS / WARP) {
+            int32_t x = fr[sd][i];
+            Row r = p.g.row[x];
+            const int32_t* rw = p.g.pool + r.start;
+            for (int b0 = 0; b0 < r.len; b0 += WARP) {
+                if (ld_volatile(&s_met) || ld_volatile(&s_over)) break;
+                int k = b0 + (int)lane_id();
+                if (k < r.len) {
+                    int32_t y = rw[k];
+                    if (hs_has(hs[sd ^ 1], y)) {
+                        s_met = 1;
+                    } else {
+                        int ins = hs_insert(hs[sd], y);
+                        if (ins < 0) s_over = 1;
+                        else if (ins == 1) {
+                            int tt = atomicAdd(&s_touched, 1) + 1;
+                            int at = atomicAdd(&s_nn, 1);
+                            if (tt > p.bound || at >= CC_FCAP) s_over = 1;
+                            else nf[at] = y;
+                        }
+                    }
+                    bytes += 8;
+                }
+            }
+        }
+        __syncthreads();
+        if (s_met) return 0;
+        if (s_over) return 2;
+        const int nn = s_nn;
+        for (int i = t; i < nn; i += CC_THREADS) fr[sd][i] = nf[i];
+        __syncthreads();
+        if (t == 0) s_fn[sd] = nn;
+        __syncthreads();
+    }
+    // one side is exhausted: its visited set is a whole component
+    const int ex = s_fn[0] == 0 ? 0 : 1;
+    __shared__ int s_size, s_min;
+    __shared__ long long s_off;
+    if (t == 0) { s_size = 0; s_min = INT32_MAX; }
+    __syncthreads();
+    for (int i = t; i < CC_HCAP; i += CC_THREADS) {
+        int32_t x = hs[ex][i];
+        if (x >= 0) { atomicAdd(&s_size, 1); atomicMin(&s_min, x); }
+    }
+    __syncthreads();
+    if (t == 0) {
+        s_off = atomicAdd((unsigned long long*)&p.ctr->aux64[0], (unsigned long long)s_size);
+        int rid = atomicAdd(&p.ctr->list_count[2], 1);
+        if (s_off + s_size > p.side_cap || 2LL * rid + 1 >= p.rec_cap) {
+            atomicExch(p.dirty + cls, p.epoch);   // no room to record the side: recompute the class
+            s_off = -1;
+        } else {
+            p.rec[2 * rid] = ((unsigned long long)(uint32_t)cls << 32) | (uint32_t)s_min;
+            p.rec[2 * rid + 1] = ((unsigned long long)s_off << 32) | (uint32_t)s_size;
+            atomicAdd(p.cnt + cls, 1);
+        }
+    }
+    __syncthreads();
+    if (s_off >= 0) {
+        __shared__ int s_w;
+        if (t == 0) s_w = 0;
+        __syncthreads();
+        for (int i = t; i < CC_HCAP; i += CC_THREADS) {
+            int32_t x = hs[ex][i];
+            if (x >= 0) p.side[s_off + atomicAdd(&s_w, 1)] = x;
+        }
+        __syncthreads();
+    }
+    return 1;
+}
+
+__global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
+    const int W = gwarp_count(), wid = gwarp_id();
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const int64_t n = p.g.n;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    const int nh = ld_volatile(&p.ctr->n_half);
+    long long bytes = 0;
+    __shared__ int s_task;
+
+    if (!p.full) {
+        // ---- P0: unions of inserted edges ---------------------------------------------------
+        for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
+            int64_t k = b + lane_id();
+            int32_t hooked = -1;
+            if (k < nh) {
+                unsigned long long key = p.hkeys[k];
+                int op = (int)((key >> p.B) & 1ull);
+                int32_t x = (int32_t)(key >> (p.B + 1));
+                int32_t y = (int32_t)(key & ((1ull << p.B) - 1));
+                if (op == 0 && x < y) hooked = uf_union(p.uf, ld_volatile(p.label + x), ld_volatile(p.label + y));
+            }
+            int at = warp_append(hooked >= 0, &p.ctr->list_count[1]);
+            if (hooked >= 0) p.merged[at] = hooked;
+        }
+        if (!grid_sync(p.bar, 30)) return;
+        const int nm = ld_volatile(&p.ctr->list_count[1]);
+        if (nm > 0) {
+            for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
+                int64_t v = b + lane_id();
+                bool ch = false;
+                if (v < n) {
+                    int32_t l = p.label[v];
+                    if (ld_volatile(p.uf + l) != l) { p.label[v] = uf_find(p.uf, l); ch = true; }
+                }
+                cc_touch(p, ch, (int32_t)v);
+            }
+            if (tid == 0) bytes += 8LL * n;
+            if (!grid_sync(p.bar, 31)) return;
+            for (int64_t i = tid; i < nm; i += T) {
+                int32_t l = p.merged[i];
+                p.uf[l] = l;
+            }
+        }
+        // ---- P1: one block per deletion -----------------------------------------------------
+        while (true) {
+            if (threadIdx.x == 0) s_task = atomicAdd(&p.ctr->list_count[3], 1);
+            __syncthreads();
+            const int k = s_task;
+            __syncthreads();
+            if (k >= nh) break;
+            unsigned long long key = p.hkeys[k];
+            int op = (int)((key >> p.B) & 1ull);
+            int32_t x = (int32_t)(key >> (p.B + 1));
+            int32_t y = (int32_t)(key & ((1ull << p.B) - 1));
+            if (op != 1 || x > y) continue;
+            int32_t cls = ld_volatile(p.label + x);
+            if (cls != ld_volatile(p.label + y)) continue;
+            if (threadIdx.x == 0) atomicAdd(&p.ctr->searches, 1);
+            int res = cc_search(p, x, y, cls, bytes);
+            if (threadIdx.x == 0 && res == 2 && atomicExch(p.dirty + cls, p.epoch) != p.epoch)
+                atomicAdd(&p.ctr->recomputes, 1);
+            __syncthreads();
+        }
+        if (!grid_sync(p.bar, 32)) return;
+        // ---- P2: single splits relabel locally; the rest are dirty ----------------------------
+        const int nrec = min(ld_volatile(&p.ctr->list_count[2]), (int)(p.rec_cap / 2));
+        for (int i = wid; i < nrec; i += W) {
+            unsigned long long r0 = p.rec[2 * i], r1 = p.rec[2 * i + 1];
+            int32_t cls = (int32_t)(r0 >> 32), mn = (int32_t)(r0 & 0xffffffffu);
+            long long off = (long long)(r1 >> 32);
+            int size = (int)(r1 & 0xffffffffu);
+            if (ld_volatile(p.dirty + cls) == p.epoch || ld_volatile(p.cnt + cls) != 1) {
+                if (lane_id() == 0 && atomicExch(p.dirty + cls, p.epoch) != p.epoch) atomicAdd(&p.ctr->recomputes, 1);
+                continue;
+            }
+            if (lane_id() == 0) {
+                atomicAdd(&p.ctr->splits, 1);
+                if (mn == cls) p.remf[cls] = p.epoch;
+            }
+            for (int b0 = 0; b0 < size; b0 += WARP) {
+                int j = b0 + (int)lane_id();
+                bool ok = j < size;
+                int32_t w = ok ? p.side[off + j] : 0;
+                bool ch = false;
+                if (ok) {
+                    p.st_side[w] = p.epoch;
+                    if (p.label[w] != mn) { p.label[w] = mn; ch = true; }
+                }
+                cc_touch(p, ch, w);
+            }
+        }
+        if (!grid_sync(p.bar, 33)) return;
+        // remainder of a class whose minimum left with the split side: its own minimum
+        for (int64_t v = tid; v < n; v += T) {
+            int32_t l = p.label[v];
+            if (ld_volatile(p.remf + l) == p.epoch && ld_volatile(p.st_side + v) != p.epoch &&
+                ld_volatile(p.dirty + l) != p.epoch)
+                atomicMin(p.newmin + l, (int32_t)v);
+        }
+        if (tid == 0) bytes += 12LL * n;
+        if (!grid_sync(p.bar, 34)) return;
+        for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
+            int64_t v = b + lane_id();
+            bool ch = false;
+            if (v < n) {
+                int32_t l = p.label[v];
+                if (ld_volatile(p.remf + l) == p.epoch && ld_volatile(p.st_side + v) != p.epoch &&
+                    ld_volatile(p.dirty + l) != p.epoch) {
+                    int32_t m = ld_volatile(p.newmin + l);
+                    if (m != l) { p.label[v] = m; ch = true; }
+                }
+            }
+            cc_touch(p, ch, (int32_t)v);
+        }
+        if (!grid_sync(p.bar, 35)) return;
+        // restore per-class scratch of split classes
+        for (int i = (int)tid; i < nrec; i += (int)T) {
+            int32_t cls = (int32_t)(p.rec[2 * i] >> 32);
+            p.cnt[cls] = 0;
+            p.newmin[cls] = INT32_MAX;
+        }
+    } else {
+        for (int64_t v = tid; v < n; v += T) {
+            p.touched[v] = (int32_t)v;
+            p.st_touch[v] = p.epoch;
+        }
+        if (leader) p.ctr->changed = (int)n;
+        if (leader) p.ctr->recomputes = 1;
+    }
+    // ---- P3: exact recompute of dirty classes (every class when full) ------------------------
+    if (!grid_sync(p.bar, 38)) return;
+    if (!p.full && ld_volatile(&p.ctr->recomputes) == 0) {
+        goto done;
+    }
+    for (int64_t v = tid; v < n; v += T) {
+        bool d = p.full || ld_volatile(p.dirty + p.label[v]) == p.epoch;
+        p.vp[v] = d ? (int32_t)v : -1;
+    }
+    if (!grid_sync(p.bar, 36)) return;
+    for (int v = wid; v < n; v += W) {   // rows up to CC_BIG: one warp each
+        if (ld_volatile(p.vp + v) < 0) continue;
+        Row r = p.g.row[v];
+        if (r.len > CC_BIG) continue;
+        const int32_t* rw = p.g.pool + r.start;
+        for (int b0 = 0; b0 < r.len; b0 += WARP) {
+            int k = b0 + (int)lane_id();
+            if (k < r.len) {
+                int32_t w = rw[k];
+                if (w > v) {
+                    // an edge leaving a dirty class means the uploaded labels did not describe
+                    // the components of the graph; flagged instead of followed
+                    if (ld_volatile(p.vp + w) < 0) atomicExch(&p.ctr->pad, 1);
+                    else uf_union(p.vp, v, w);
+                }
+            }
+        }
+        if (lane_id() == 0) bytes += 8LL * r.len;
+    }
+    for (int v = blockIdx.x; v < n; v += gridDim.x) {   // longer rows: one block each
+        if (ld_volatile(p.vp + v) < 0) continue;
+        Row r = p.g.row[v];
+        if (r.len <= CC_BIG) continue;
+        const int32_t* rw = p.g.pool + r.start;
+        for (long long k = threadIdx.x; k < r.len; k += CC_THREADS) {
+            int32_t w = rw[k];
+            if (w > v) {
+                if (ld_volatile(p.vp + w) < 0) atomicExch(&p.ctr->pad, 1);
+                else uf_union(p.vp, v, w);
+            }
+        }
+        if (threadIdx.x == 0) bytes += 8LL * r.len;
+    }
+    if (!grid_sync(p.bar, 37)) return;
+    for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
+        int64_t v = b + lane_id();
+        bool ch = false;
+        if (v < n && ld_volatile(p.vp + v) >= 0) {
+            int32_t root = uf_find(p.vp, (int32_t)v);
+            if (p.label[v] != root) { p.label[v] = root; ch = true; }
+        }
+        if (!p.full) cc_touch(p, ch, (int32_t)v);
+    }
+    if (tid == 0) bytes += 16LL * n;
+done:
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+    if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
+    if (leader) p.ctr->affected = p.ctr->changed;
+}
+
+__global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, int32_t* __restrict__ newmin, int64_t n) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        uf[v] = (int32_t)v;
+        cnt[v] = 0;
+        newmin[v] = INT32_MAX;
+    }
+}
+
+static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
+    SCOUT_RC(lists_ensure(c));
+    const int64_t n = c->n;
+    if (!c->d_misc || c->cap_misc < 6 * n) {   // uf, cnt, dirty, remf, newmin, vp
+        if (c->d_misc) dev_free(c, c->d_misc, (size_t)c->cap_misc * 4);
+        c->d_misc = nullptr;
+        c->cap_misc = 0;
+        SCOUT_RC(dev_alloc(c, &c->d_misc, (size_t)6 * n * 4, "component scratch"));
+        c->cap_misc = 6 * n;
+        SCOUT_CU(c, cudaMemsetAsync(c->d_misc, 0, (size_t)6 * n * 4, c->s_main));
+        int32_t* base = (int32_t*)c->d_misc;
+        k_cc_init<<<blocks_for(n, 256), 256, 0, c->s_main>>>(base, base + n, base + 4 * n, n);
+        SCOUT_LAUNCH(c, "k_cc_init");
+    }
+    int32_t* base = (int32_t*)c->d_misc;
+    CcParams p;
+    p.g = dgraph(c);
+    p.label = c->label;
+    p.hkeys = c->d_hkeys;
+    p.B = c->key_bits;
+    p.uf = base;
+    p.cnt = base + n;
+    p.dirty = base + 2 * n;
+    p.remf = base + 3 * n;
+    p.newmin = base + 4 * n;
+    p.vp = base + 5 * n;
+    p.merged = c->d_list[1];
+    p.rec = (unsigned long long*)c->d_qbuf[0];
+    p.rec_cap = c->qcap;
+    p.side = (int32_t*)c->d_qbuf[1];
+    p.side_cap = 2 * c->qcap;
+    p.touched = c->d_list[0];
+    p.st_touch = c->stamp_b;
+    p.st_side = c->stamp_a;
+    p.epoch = (int32_t)c->epoch;
+    // Search bound: the reference's rule is 5000, or unbounded below average degree 10;
+    // shared memory caps it here, and a search that gives up only costs a class recompute.
+    int64_t bound = sched && sched->search_bound > 0 ? sched->search_bound : 5000;
+    p.bound = (int)std::min<int64_t>(bound, CC_MAX_BOUND);
+    p.full = full;
+    p.ctr = c->d_ctr;
+    p.bar = c->d_bar;
+    static bool attr = false;
+    if (!attr) {
+        SCOUT_CU(c, cudaFuncSetAttribute(k_cc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CC_SMEM));
+        attr = true;
+    }
+    void* args[] = {&p};
+    return coop_launch(c, (const void*)k_cc, CC_THREADS, args, CC_SMEM);
+}
+
+int cc_repair(scout_ctx* c, const scout_sched* sched, scout_batch_stats* st) {
+    (void)st;
+    int full = sched && sched->mode == SCOUT_MODE_RECOMPUTE ? 1 : 0;
+    return cc_launch(c, sched, full);
+}
+
+int cc_recompute(scout_ctx* c, scout_batch_stats* st) {
+    (void)st;
+    return cc_launch(c, nullptr, 1);
+}
+
+}  // namespace scout

@@ -58,6 +58,9 @@ struct scout_ctx {
     int32_t* pool = nullptr;
     int64_t pool_cap = 0;
     int64_t tail = 0;          // first free pool element (host view)
+    int32_t* spare = nullptr;  // previous pool, next compaction target
+    int64_t spare_cap = 0;
+    int64_t compactions = 0;
     bool reserved = false;
     bool sealed = false;
     int32_t* d_tmp_rows = nullptr;   // staging target for rows of one slot
@@ -128,6 +131,7 @@ struct scout_ctx {
     int64_t last_half = 0;
     int64_t last_aff = 0;
     int32_t coop_blocks = 0;   // resident blocks of the persistent kernels
+    int64_t nlaunch = 0;       // kernels launched (running count)
 
     int fail(int code, const std::string& msg) { err = msg; return code; }
 };

@@ -197,38 +197,59 @@ __device__ __forceinline__ long long ub_keys(KeySpan s, long long n, int32_t x) 
     return lo;
 }
 
-// Per affected row (one warp): matched-deletion prefix over D (stored in mdp, aligned with the
-// keys), new length, and the small/large split.
-__global__ void k_row_plan(DGraph g, const unsigned long long* __restrict__ keys, int B,
+// Per affected row (one warp). Multiset rule: the r-th copy of d in the deletion list cancels
+// the r-th copy of d in the old row (DeltaOverlay::removeEdge forgets one added copy or
+// tombstones the base edge, FlashGraph.h:236-243). The warp finds the old entry every
+// deletion cancels, the final position of every insertion (j + #old <= y - #cancelled <= y),
+// the new length, and only then tombstones the cancelled entries (-1) in the old row, so the
+// merge kernels stream the old row without searching it. pos is aligned with the keys.
+__global__ void k_row_plan(DGraph g, int32_t* __restrict__ pool_rw, const unsigned long long* __restrict__ keys, int B,
                            DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
                            const int64_t* __restrict__ seg, int64_t* __restrict__ new_len,
-                           long long* __restrict__ mdp, int32_t* __restrict__ small_list,
-                           int32_t* __restrict__ large_list) {
+                           long long* __restrict__ mdp, long long* __restrict__ pos,
+                           int32_t* __restrict__ small_list, int32_t* __restrict__ large_list) {
     const int A = ctr->n_aff;
     for (int a = gwarp_id(); a < A; a += gwarp_count()) {
         int32_t u = aff[a];
         long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
         Row r = g.row[u];
         const int32_t* O = g.pool + r.start;
+        KeySpan I{keys + b0, B};
         KeySpan D{keys + sp, B};
         long long q = e0 - sp, p = sp - b0;
         long long run = 0;
         for (long long base = 0; base < q; base += WARP) {
             long long k = base + lane_id();
             int matched = 0;
+            long long at = -1;
             if (k < q) {
                 int32_t d = D[k];
                 long long rank = k - lb_keys(D, q, d);
-                matched = rank < count_in(O, r.len, d) ? 1 : 0;
+                long long lo = lower_bound_i32(O, r.len, d);
+                long long cnt = upper_bound_i32(O + lo, r.len - lo, d);
+                if (rank < cnt) { matched = 1; at = lo + rank; }
             }
             int inc = warp_incl_scan_i(matched);
-            if (k < q) mdp[sp + k] = run + inc;
+            if (k < q) { mdp[sp + k] = run + inc; pos[sp + k] = at; }
             run += __shfl_sync(0xffffffffu, inc, WARP - 1);
+        }
+        __syncwarp();
+        for (long long j = lane_id(); j < p; j += WARP) {
+            int32_t y = I[j];
+            long long ubo = upper_bound_i32(O, r.len, y);
+            long long ubd = ub_keys(D, q, y);
+            long long del = ubd > 0 ? mdp[sp + ubd - 1] : 0;
+            pos[b0 + j] = j + ubo - del;
+        }
+        __syncwarp();
+        for (long long k = lane_id(); k < q; k += WARP) {
+            long long at = pos[sp + k];
+            if (at >= 0) pool_rw[r.start + at] = -1;
         }
         if (lane_id() == 0) {
             long long nl = (long long)r.len + p - run;
             new_len[a] = nl;
-            long long work = (long long)r.len + p + q;
+            long long work = (long long)r.len + p;
             if (work <= SMALL_ROW_LIMIT) small_list[atomicAdd(&ctr->n_small, 1)] = a;
             else large_list[atomicAdd(&ctr->n_large, 1)] = a;
             atomicAdd((unsigned long long*)&ctr->nnz_delta, (unsigned long long)(nl - r.len));
@@ -238,45 +259,44 @@ __global__ void k_row_plan(DGraph g, const unsigned long long* __restrict__ keys
     }
 }
 
-// Output position of old element O[i] (a survivor): survivors before i plus insertions < x.
-// Position of insertion I[j]: j + survivors <= I[j] = j + ub(O, y) - mdp(ub(D, y)).
+// Streams a tombstoned old row into its new place: survivor i lands at (#survivors before i)
+// + (#insertions < x); the insertion count is searched only inside the range spanned by the
+// warp's current values, which is almost always empty.
 template <int GROUP>
-__device__ __forceinline__ void merge_row(int tid, Row r, const int32_t* __restrict__ pool_in, int32_t* __restrict__ out,
-                                          KeySpan I, long long p, KeySpan D, long long q,
-                                          const long long* __restrict__ mdp_d, long long* s_run, unsigned* s_cnt) {
-    const int32_t* O = pool_in + r.start;
-    // Insertions first (independent of the survivor scan).
-    for (long long j = tid; j < p; j += GROUP) {
-        int32_t y = I[j];
-        long long ubo = upper_bound_i32(O, r.len, y);
-        long long ubd = ub_keys(D, q, y);
-        long long del = ubd > 0 ? mdp_d[ubd - 1] : 0;
-        out[j + ubo - del] = y;
-    }
-    // Old elements in chunks of GROUP with a running survivor count.
+__device__ __forceinline__ void merge_stream(int tid, const int32_t* __restrict__ O, long long len,
+                                             int32_t* __restrict__ out, KeySpan I, long long p,
+                                             long long* s_run, unsigned* s_cnt) {
     long long run = 0;
-    for (long long base = 0; base < r.len; base += GROUP) {
+    for (long long base = 0; base < len; base += GROUP) {
         long long i = base + tid;
-        bool surv = false;
-        int32_t x = 0;
-        if (i < r.len) {
-            x = O[i];
-            long long cd = q ? (ub_keys(D, q, x) - lb_keys(D, q, x)) : 0;
-            if (cd == 0) surv = true;
-            else {
-                long long rnk = i - lower_bound_i32(O, r.len, x);
-                surv = rnk >= cd;
+        int32_t x = i < len ? O[i] : -1;
+        bool surv = x >= 0;
+        long long lbI = 0;
+        if (p > 0) {
+            int xmin = __reduce_min_sync(0xffffffffu, surv ? x : INT32_MAX);
+            int xmax = __reduce_max_sync(0xffffffffu, surv ? x : -1);
+            long long cl = 0, ch = 0;
+            if (xmax >= 0 && lane_id() == 0) {
+                cl = lb_keys(I, p, xmin);
+                ch = lb_keys(I, p, xmax);
+            }
+            cl = __shfl_sync(0xffffffffu, cl, 0);
+            ch = __shfl_sync(0xffffffffu, ch, 0);
+            if (surv) {
+                long long lo = cl, hi = ch;
+                while (lo < hi) {
+                    long long mid = (lo + hi) >> 1;
+                    if (I[mid] < x) lo = mid + 1; else hi = mid;
+                }
+                lbI = lo;
             }
         }
-        long long before;
-        long long chunk_total;
+        unsigned m = __ballot_sync(0xffffffffu, surv);
+        long long before, chunk_total;
         if (GROUP == WARP) {
-            unsigned m = __ballot_sync(0xffffffffu, surv);
             before = __popc(m & ((1u << lane_id()) - 1));
             chunk_total = __popc(m);
         } else {
-            // block-wide exclusive count via per-warp ballots
-            unsigned m = __ballot_sync(0xffffffffu, surv);
             int w = tid / WARP;
             if (lane_id() == 0) s_cnt[w] = __popc(m);
             __syncthreads();
@@ -290,10 +310,7 @@ __device__ __forceinline__ void merge_row(int tid, Row r, const int32_t* __restr
             chunk_total = *s_run;
             __syncthreads();
         }
-        if (surv) {
-            long long pos = run + before + lb_keys(I, p, x);
-            out[pos] = x;
-        }
+        if (surv) out[run + before + lbI] = x;
         run += chunk_total;
     }
 }
@@ -301,17 +318,18 @@ __device__ __forceinline__ void merge_row(int tid, Row r, const int32_t* __restr
 __global__ void k_merge_small(Row* __restrict__ row, const int32_t* __restrict__ pool_in, int32_t* __restrict__ pool_out,
                               const unsigned long long* __restrict__ keys, int B, const DevCounters* __restrict__ ctr,
                               const int32_t* __restrict__ aff, const int64_t* __restrict__ seg,
-                              const int64_t* __restrict__ off, const long long* __restrict__ mdp,
+                              const int64_t* __restrict__ off, const long long* __restrict__ pos,
                               const int32_t* __restrict__ list, long long tail) {
     const int cnt = ctr->n_small;
     for (int k = gwarp_id(); k < cnt; k += gwarp_count()) {
         int a = list[k];
         int32_t u = aff[a];
-        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
         Row r = row[u];
         long long start = tail + off[a];
-        merge_row<WARP>(lane_id(), r, pool_in, pool_out + start, KeySpan{keys + b0, B}, sp - b0, KeySpan{keys + sp, B},
-                        e0 - sp, mdp + sp, nullptr, nullptr);
+        KeySpan I{keys + b0, B};
+        for (long long j = lane_id(); j < sp - b0; j += WARP) pool_out[start + pos[b0 + j]] = I[j];
+        merge_stream<WARP>(lane_id(), pool_in + r.start, r.len, pool_out + start, I, sp - b0, nullptr, nullptr);
         __syncwarp();
         int nl = (int)(off[a + 1] - off[a]);
         if (lane_id() == 0) row[u] = Row{start, nl, nl};
@@ -321,7 +339,7 @@ __global__ void k_merge_small(Row* __restrict__ row, const int32_t* __restrict__
 __global__ void k_merge_large(Row* __restrict__ row, const int32_t* __restrict__ pool_in, int32_t* __restrict__ pool_out,
                               const unsigned long long* __restrict__ keys, int B, const DevCounters* __restrict__ ctr,
                               const int32_t* __restrict__ aff, const int64_t* __restrict__ seg,
-                              const int64_t* __restrict__ off, const long long* __restrict__ mdp,
+                              const int64_t* __restrict__ off, const long long* __restrict__ pos,
                               const int32_t* __restrict__ list, long long tail) {
     __shared__ long long s_run;
     __shared__ unsigned s_cnt[LARGE_THREADS / WARP];
@@ -329,11 +347,12 @@ __global__ void k_merge_large(Row* __restrict__ row, const int32_t* __restrict__
     for (int k = blockIdx.x; k < cnt; k += gridDim.x) {
         int a = list[k];
         int32_t u = aff[a];
-        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
         Row r = row[u];
         long long start = tail + off[a];
-        merge_row<LARGE_THREADS>(threadIdx.x, r, pool_in, pool_out + start, KeySpan{keys + b0, B}, sp - b0,
-                                 KeySpan{keys + sp, B}, e0 - sp, mdp + sp, &s_run, s_cnt);
+        KeySpan I{keys + b0, B};
+        for (long long j = threadIdx.x; j < sp - b0; j += LARGE_THREADS) pool_out[start + pos[b0 + j]] = I[j];
+        merge_stream<LARGE_THREADS>(threadIdx.x, pool_in + r.start, r.len, pool_out + start, I, sp - b0, &s_run, s_cnt);
         __syncthreads();
         int nl = (int)(off[a + 1] - off[a]);
         if (threadIdx.x == 0) row[u] = Row{start, nl, nl};
@@ -437,6 +456,9 @@ int counters_fetch(scout_ctx* c) {
     SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
     if (c->h_bar->err == 1)
         return c->fail(SCOUT_E_TIMEOUT, "a device grid barrier timed out (tag " + std::to_string(c->h_bar->where) + ")");
+    if (c->h_ctr->pad)
+        return c->fail(SCOUT_E_STATE, "the component labels do not describe the components of the graph "
+                                      "(an edge joins two labels); upload a consistent labelling");
     if (c->h_bar->err != 0 || c->h_ctr->overflow)
         return c->fail(SCOUT_E_CAPACITY, "a device work list overflowed its capacity");
     return SCOUT_OK;
@@ -469,15 +491,34 @@ int graph_compact(scout_ctx* c, int64_t min_free) {
         if (cudaStreamSynchronize(c->s_main) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "compaction");
     }
     int64_t cap = std::max<int64_t>(c->pool_cap, live + min_free);
+    // Ping-pong: the previous pool is kept as the next compaction's target, so steady-state
+    // compactions allocate nothing. Without budget room for two pools the old one is freed.
     int32_t* np = nullptr;
-    if (rc == SCOUT_OK) rc = dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool");
+    if (rc == SCOUT_OK) {
+        if (c->spare && c->spare_cap >= cap) {
+            np = c->spare;
+            cap = c->spare_cap;
+            c->spare = nullptr;
+            c->spare_cap = 0;
+        } else {
+            if (c->spare) { dev_free(c, c->spare, (size_t)c->spare_cap * 4); c->spare = nullptr; c->spare_cap = 0; }
+            rc = dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool");
+        }
+    }
     if (rc != SCOUT_OK) { dev_free(c, off, (size_t)(n + 1) * 8); return rc; }
     k_copy_rows<<<blocks_for(n * WARP, 256), 256, 0, c->s_main>>>(c->row, c->pool, np, off, (int32_t)n);
     k_rows_compacted<<<nb, 256, 0, c->s_main>>>(c->row, off, (int32_t)n);
     SCOUT_LAUNCH(c, "compaction");
+    c->nlaunch += 5;
     SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
-    dev_free(c, c->pool, (size_t)c->pool_cap * sizeof(int32_t));
     dev_free(c, off, (size_t)(n + 1) * 8);
+    if (c->held <= c->budget / 100 * 85) {   // keep the old pool as the next target
+        c->spare = c->pool;
+        c->spare_cap = c->pool_cap;
+    } else {
+        dev_free(c, c->pool, (size_t)c->pool_cap * sizeof(int32_t));
+    }
+    c->compactions++;
     c->pool = np;
     c->pool_cap = cap;
     c->tail = live;
@@ -509,12 +550,18 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_RC(ws_ensure(c, m));
     SCOUT_RC(graph_ensure_scratch(c));
     if (st) st->h2d_bytes += m * (int64_t)sizeof(scout_edge) + (ops ? m : 0);
-    if (m == 0) { c->d_hkeys = c->d_keys; return SCOUT_OK; }
+    if (m == 0) {
+        c->d_hkeys = c->d_keys;
+        SCOUT_CU(c, cudaEventRecord(c->ev_t[3], c->s_main));
+        return SCOUT_OK;
+    }
     SCOUT_RC(upload_edits(c, edits, ops, m));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[3], c->s_main));
     DGraph g = dgraph(c);
     k_classify<<<blocks_for(m, 256), 256, 0, c->s_main>>>(g, c->d_edits, ops ? c->d_ops : nullptr, m, B, c->d_keys,
                                                          c->d_eflag, c->d_ctr, 1);
     SCOUT_LAUNCH(c, "k_classify");
+    c->nlaunch += 1;
     unsigned long long* sorted = nullptr;
     SCOUT_RC(sort_keys(c, c->d_keys, c->d_keys_alt, 2 * m, 2 * B + 1, &sorted));
     c->d_hkeys = sorted;
@@ -524,21 +571,25 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     k_seg_heads<<<nbh, 256, 0, c->s_main>>>(sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->aux_w);
     k_seg_tails<<<nbh, 256, 0, c->s_main>>>(sorted, B, c->d_ctr, c->d_aff_seg, c->aux_w);
     SCOUT_LAUNCH(c, "segments");
+    c->nlaunch += 2;
     SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
-    k_row_plan<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(g, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg,
-                                                                     c->d_aff_len, c->d_mdp, c->d_aff_small,
-                                                                     c->d_aff_large);
+    long long* pos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
+    k_row_plan<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(g, c->pool, sorted, B, c->d_ctr, c->d_aff,
+                                                                     c->d_aff_seg, c->d_aff_len, c->d_mdp, pos,
+                                                                     c->d_aff_small, c->d_aff_large);
     SCOUT_LAUNCH(c, "k_row_plan");
+    c->nlaunch += 1;
     // Exclusive scan over Amax + 1 entries (the tail entries are zero), so the new length of
     // affected row a is off[a + 1] - off[a] for every a.
     SCOUT_RC(scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems));
     k_merge_small<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(
-        c->row, c->pool, c->pool, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len, c->d_mdp,
+        c->row, c->pool, c->pool, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len, pos,
         c->d_aff_small, (long long)c->tail);
     k_merge_large<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(Amax, 4 * c->sm_count)), LARGE_THREADS, 0,
                     c->s_main>>>(c->row, c->pool, c->pool, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len,
-                                 c->d_mdp, c->d_aff_large, (long long)c->tail);
+                                 pos, c->d_aff_large, (long long)c->tail);
     SCOUT_LAUNCH(c, "merge");
+    c->nlaunch += 2;
     return SCOUT_OK;
 }
 
@@ -556,7 +607,10 @@ int scout_graph_reserve(scout_ctx* c, int64_t n, int64_t nnz) {
     c->n = n;
     SCOUT_RC(dev_alloc(c, (void**)&c->row, (size_t)n * sizeof(Row), "row table"));
     SCOUT_CU(c, cudaMemsetAsync(c->row, 0, (size_t)n * sizeof(Row), c->s_main));
-    c->pool_cap = 2 * nnz + (1 << 22);
+    // Room for several batches of rewritten rows between compactions (HBM is plentiful; a
+    // budget that cannot hold four times the graph falls back to twice).
+    c->pool_cap = 4 * nnz + (1 << 26);
+    if ((uint64_t)c->pool_cap * 4 * 2 + c->held > c->budget) c->pool_cap = 2 * nnz + (1 << 22);
     SCOUT_RC(dev_alloc(c, (void**)&c->pool, (size_t)c->pool_cap * sizeof(int32_t), "element pool"));
     c->tail = 0;
     c->nnz = 0;
@@ -688,7 +742,7 @@ int scout_graph_seal(scout_ctx* c) {
     dev_free(c, flags, 16);
     SCOUT_LAUNCH(c, "seal");
     // Contiguous rows, exact nnz and tail.
-    SCOUT_RC(graph_compact(c, std::max<int64_t>(c->pool_cap / 2, 1 << 22)));
+    SCOUT_RC(graph_compact(c, std::max<int64_t>(c->pool_cap - c->tail, 1 << 22)));
     c->sealed = true;
     return SCOUT_OK;
 }

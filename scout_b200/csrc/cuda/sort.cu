@@ -163,6 +163,7 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
         }
         k_sort_small<<<1, SMALL_SORT_THREADS, smem, c->s_main>>>(keys, (int)n, bits);
         SCOUT_LAUNCH(c, "k_sort_small");
+        c->nlaunch += 1;
         return SCOUT_OK;
     }
     int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
@@ -174,6 +175,7 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
         k_scan_u32_single<<<1, 1024, 0, c->s_main>>>(c->d_sort_hist, (int64_t)nblocks * SORT_RADIX);
         k_sort_scatter<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, dst, n, shift, c->d_sort_hist, nblocks);
         SCOUT_LAUNCH(c, "radix pass");
+        c->nlaunch += 3;
         unsigned long long* s = src; src = dst; dst = s;
     }
     *sorted_out = src;
@@ -266,6 +268,7 @@ int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total) {
     k_scan_sums<<<1, 1024, 0, c->s_main>>>(c->d_scan_tmp, nb, d_total);
     k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
     SCOUT_LAUNCH(c, "scan_i64");
+    c->nlaunch += 3;
     return SCOUT_OK;
 }
 
