@@ -175,6 +175,23 @@ int scout_recompute_cc(scout_ctx* ctx, scout_batch_stats* stats);
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 
+/* ---- allocation-free entry point ------------------------------------------------------ */
+/* No counterpart in the reference. BFS levels from `source` (-1 unreached) over a CSR that
+ * the caller already holds in device memory (d_off: n + 1 int64 offsets, d_adj: int32
+ * neighbours), written to the caller's device buffer d_level (n int32), on the caller's
+ * stream (a cudaStream_t, NULL for the default stream); returns when the levels are ready.
+ * It allocates nothing: for callers that cannot call cudaMalloc (code running while a CUDA
+ * graph is being captured, runtimes whose device memory belongs to another allocator or a
+ * fixed arena, real-time loops that must stay off the driver's allocator). Its working
+ * buffers live in one static device array of 8 MB that every GPU loading the library keeps
+ * until the process exits, which bounds n to 1,048,576 vertices; larger graphs are refused
+ * with SCOUT_E_CAPACITY. The first call on a device looks up that array's device address,
+ * so make it before any stream capture. All calls share the array: calls that overlap on
+ * the GPU (two host threads, or two streams) race and must be serialised by the caller.
+ * No context is involved; errors are reported through scout_last_error(NULL). */
+int scout_bfs_levels_noalloc(const int64_t* d_off, const int32_t* d_adj, int64_t n, int32_t source,
+                             int32_t* d_level, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,7 @@ SIGNATURES = [
     ("scout_recompute_bfs", C.c_int, [_vp, C.c_int32, C.POINTER(ScoutBatchStats)]),
     ("scout_recompute_cc", C.c_int, [_vp, C.POINTER(ScoutBatchStats)]),
     ("scout_sync", C.c_int, [_vp, C.c_int64]),
+    ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h
     ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
     ("scout_egr_close", C.c_int, [_vp]),
@@ -129,4 +130,16 @@ def load() -> C.CDLL:
     return lib
 
 
-LIB = load()
+class _Lazy:
+    """Loads libscout.so on first use, so the package (and its build recipe) imports before
+    the library exists; any call without the built library raises ImportError."""
+
+    _lib = None
+
+    def __getattr__(self, name):
+        if _Lazy._lib is None:
+            _Lazy._lib = load()
+        return getattr(_Lazy._lib, name)
+
+
+LIB = _Lazy()

@@ -156,6 +156,7 @@ int dev_grow(scout_ctx* c, T** p, int64_t* cap, int64_t need, const char* what) 
 int pin_grow(scout_ctx* c, void** p, int64_t* cap_bytes, int64_t need_bytes);
 
 int cuda_fail(scout_ctx* c, cudaError_t e, const char* where);
+int host_fail(int code, const std::string& msg);   // thread-local message for calls without a context
 #define SCOUT_CU(c, call)                                                  \
     do {                                                                   \
         cudaError_t e_ = (call);                                           \
