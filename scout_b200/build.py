@@ -101,7 +101,8 @@ def build_cli(force: bool = False) -> list[str]:
     for p in ("mis", "coloring", "bfs", "cc"):
         out = os.path.join(BINDIR, f"scout_{p}")
         if force or _stale(out, [src, lib] + _headers()):
-            _run([CXX] + CXXFLAGS + [f"-DSCOUT_PROBLEM_NAME=\"{p}\"", src, "-o", out, f"-L{LIBDIR}", "-lscout",
+            flags = [f for f in CXXFLAGS if f != "-fopenmp"]   # the CLI itself has no OpenMP region
+            _run([CXX] + flags + [f"-DSCOUT_PROBLEM_NAME=\"{p}\"", src, "-o", out, f"-L{LIBDIR}", "-lscout",
                                      f"-Wl,-rpath,{LIBDIR}", "-Wl,-rpath,$ORIGIN/../scout_b200/lib"])
         outs.append(out)
     return outs
