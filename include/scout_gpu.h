@@ -64,7 +64,9 @@ typedef struct scout_sched {
     int32_t frontier;         /* scout_frontier                                     */
     int32_t lanes_per_vertex; /* 0 auto; else 1, 2, 4, 8, 32                         */
     int64_t search_bound;     /* CC local-search bound (vertices); 0 = reference rule */
-    int64_t reserved[4];
+    int64_t search_limit;     /* CC: a class with more deletions left to search than this is
+                                 recomputed instead (0 = 32; < 0 = always search)        */
+    int64_t reserved[3];
 } scout_sched;
 
 /* Per-batch statistics (the fields of the reference's Stats structs, scout_bfs.cu:417-424,
@@ -92,7 +94,8 @@ typedef struct scout_batch_stats {
     int64_t update_bytes; /* algorithmic HBM bytes of the row merge                   */
     int64_t launches;     /* kernels launched by the call                             */
     double  ms_h2d;       /* device: copy of the edits into HBM                       */
-    int64_t reserved[5];
+    double  phase_ms[4];  /* device: duration of the repair kernel's first four phases   */
+    int64_t reserved[1];
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;

@@ -27,7 +27,8 @@ class ScoutEdge(C.Structure):
 
 class ScoutSched(C.Structure):
     _fields_ = [("policy", C.c_int32), ("mode", C.c_int32), ("frontier", C.c_int32),
-                ("lanes_per_vertex", C.c_int32), ("search_bound", C.c_int64), ("reserved", C.c_int64 * 4)]
+                ("lanes_per_vertex", C.c_int32), ("search_bound", C.c_int64), ("search_limit", C.c_int64),
+                ("reserved", C.c_int64 * 3)]
 
 
 class ScoutBatchStats(C.Structure):
@@ -38,10 +39,12 @@ class ScoutBatchStats(C.Structure):
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("ms_update", C.c_double),
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
                 ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
-                ("reserved", C.c_int64 * 5)]
+                ("phase_ms", C.c_double * 4), ("reserved", C.c_int64 * 1)]
 
     def as_dict(self) -> dict:
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("reserved", "phase_ms")}
+        d["phase_ms"] = list(self.phase_ms)
+        return d
 
 
 _vp = C.c_void_p

@@ -71,7 +71,7 @@ static void release(scout_ctx* c) {
     for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
     void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
-                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_misc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
+                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_misc, c->d_cc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
                     c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
     for (void* p : devs) if (p) cudaFree(p);
     void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
@@ -291,6 +291,10 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     st->ms_h2d = ev_ms(c->ev_t[0], c->ev_t[3]);
     st->ms_update = ev_ms(c->ev_t[3], c->ev_t[1]);
     st->launches = c->nlaunch - launch0;
+    for (int i = 0; i < 4; i++) {
+        unsigned long long a = h.phase_ns[i], b = h.phase_ns[i + 1];
+        st->phase_ms[i] = (a && b && b >= a) ? (double)(b - a) / 1e6 : 0.0;
+    }
     st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
     c->last_changed = h.changed;
     st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

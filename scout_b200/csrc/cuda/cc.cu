@@ -7,14 +7,17 @@
 // the stream (516-527). Here every batch ends with the exact partition:
 //   P0  inserted edges hook label roots in a union-find over labels (lower root wins), then
 //       every vertex takes its root, which is the minimum vertex id of the merged class
-//   P1  each deletion gets one block: common-neighbour check, then the bounded bidirectional
-//       search in shared-memory hash sets (the reference's rule, expanded in parallel);
-//       outcomes: connected, split (the exhausted side is a whole component), inconclusive
-//   P2  a class with exactly one split and no inconclusive search splits in two: the side gets
-//       its minimum id as label; when the side holds the class minimum, the remainder gets
-//       its own minimum. A class with more outcomes is marked dirty
-//   P3  dirty classes are recomputed exactly: CAS union-find (lower root wins) over the rows
-//       of their vertices, then label = root
+//   P1a one warp per deletion: a common neighbour settles it. A class left with more than
+//       the search limit of unsettled deletions is marked dirty (one recompute of the class
+//       is cheaper than that many searches)
+//   P1b one block per remaining deletion: the bounded bidirectional search in shared-memory
+//       hash sets (the reference's rule, expanded in parallel); outcomes: connected, split
+//       (the exhausted side is a whole component), inconclusive (class marked dirty)
+//   P2  split sides take their minimum id as label; when a side holds the class minimum, the
+//       remainder gets its own minimum. With several splits in a class the remainder must be
+//       shown connected first (endpoint searches); otherwise the class is marked dirty
+//   P3  dirty classes are recomputed exactly (Afforest-style: link the first two neighbours,
+//       compress, sample the dominant root, union the rest of the rows of the others)
 // A full recompute (scout_recompute_cc) is P3 with every class dirty. One cooperative launch,
 // phases separated by the bounded grid barrier.
 #include "ctx.cuh"
@@ -39,6 +42,11 @@ struct CcParams {
     int32_t* remf;      // == epoch: class remainder needs its new minimum
     int32_t* newmin;    // remainder minimum per class (INT32_MAX at rest)
     int32_t* vp;        // vertex union-find for recomputes
+    int32_t* firstw;    // first surviving split endpoint per class (-1 at rest)
+    int32_t* hard;      // deletions left to the block searches (half-edit indices)
+    int hard_cap;
+    int32_t* hcnt;      // deletions left to search, per class (zero at rest)
+    int search_limit;   // above this many per class, the class is recomputed instead
     int32_t* merged;    // labels hooked this batch (n)
     unsigned long long* rec;   // split records: (class << 32 | min), (offset << 32 | size)
     int64_t rec_cap;
@@ -109,7 +117,7 @@ __device__ __forceinline__ int hs_insert(int32_t* hs, int32_t x) {
 
 // Bounded bidirectional search of one deletion (u, v) by the whole block.
 // Returns 0 connected, 1 split (side written to p.side), 2 inconclusive.
-__device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, long long& bytes) {
+__device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, long long& bytes, bool record) {
     extern __shared__ int32_t sm[];
     int32_t* hs[2] = {sm, sm + CC_HCAP};
     int32_t* fr[2] = {sm + 2 * CC_HCAP, sm + 2 * CC_HCAP + CC_FCAP};
@@ -134,6 +142,7 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
     if (s_met) return 0;
     for (int i = t; i < 2 * CC_HCAP; i += CC_THREADS) sm[i] = -1;
     __syncthreads();
+    __shared__ long long s_vol[2], s_nvol;
     if (t == 0) {
         hs_insert(hs[0], u);
         hs_insert(hs[1], v);
@@ -141,15 +150,20 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
         fr[1][0] = v;
         s_fn[0] = 1;
         s_fn[1] = 1;
+        s_vol[0] = p.g.row[u].len;
+        s_vol[1] = p.g.row[v].len;
         s_touched = 2;
         s_met = 0;
         s_over = 0;
     }
     __syncthreads();
     while (s_fn[0] > 0 && s_fn[1] > 0) {
-        const int sd = s_fn[0] <= s_fn[1] ? 0 : 1;   // expand the smaller frontier
+        // Expand the side whose frontier has fewer adjacency entries to scan (the reference
+        // compares vertex counts; the volume keeps a hub endpoint from being expanded while
+        // its partner's side is still small, which is what overruns the bound).
+        const int sd = s_vol[0] <= s_vol[1] ? 0 : 1;
         const int fn = s_fn[sd];
-        if (t == 0) s_nn = 0;
+        if (t == 0) { s_nn = 0; s_nvol = 0; }
         __syncthreads();
         // warp per frontier vertex, lanes over its row
         for (int i = t / WARP; i < fn; i += CC_THREADS / WARP) {
@@ -161,7 +175,9 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
                 int k = b0 + (int)lane_id();
                 if (k < r.len) {
                     int32_t y = rw[k];
-                    if (hs_has(hs[sd ^ 1], y)) {
+                    // meet: y already reached by the other side, or adjacent to its endpoint
+                    // (a binary search that stands in for the other side's first level)
+                    if (hs_has(hs[sd ^ 1], y) || dg_adjacent(p.g, y, sd == 0 ? v : u)) {
                         s_met = 1;
                     } else {
                         int ins = hs_insert(hs[sd], y);
@@ -170,7 +186,10 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
                             int tt = atomicAdd(&s_touched, 1) + 1;
                             int at = atomicAdd(&s_nn, 1);
                             if (tt > p.bound || at >= CC_FCAP) s_over = 1;
-                            else nf[at] = y;
+                            else {
+                                nf[at] = y;
+                                atomicAdd((unsigned long long*)&s_nvol, (unsigned long long)p.g.row[y].len);
+                            }
                         }
                     }
                     bytes += 8;
@@ -183,7 +202,7 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
         const int nn = s_nn;
         for (int i = t; i < nn; i += CC_THREADS) fr[sd][i] = nf[i];
         __syncthreads();
-        if (t == 0) s_fn[sd] = nn;
+        if (t == 0) { s_fn[sd] = nn; s_vol[sd] = s_nvol; }
         __syncthreads();
     }
     // one side is exhausted: its visited set is a whole component
@@ -197,15 +216,18 @@ __device__ int cc_search(const CcParams& p, int32_t u, int32_t v, int32_t cls, l
         if (x >= 0) { atomicAdd(&s_size, 1); atomicMin(&s_min, x); }
     }
     __syncthreads();
+    if (!record) return 1;
     if (t == 0) {
         s_off = atomicAdd((unsigned long long*)&p.ctr->aux64[0], (unsigned long long)s_size);
         int rid = atomicAdd(&p.ctr->list_count[2], 1);
-        if (s_off + s_size > p.side_cap || 2LL * rid + 1 >= p.rec_cap) {
-            atomicExch(p.dirty + cls, p.epoch);   // no room to record the side: recompute the class
+        if (s_off + s_size > p.side_cap || 3LL * rid + 2 >= p.rec_cap) {
+            // no room to record the side: recompute the class
+            if (atomicExch(p.dirty + cls, p.epoch) != p.epoch) atomicAdd(&p.ctr->recomputes, 1);
             s_off = -1;
         } else {
-            p.rec[2 * rid] = ((unsigned long long)(uint32_t)cls << 32) | (uint32_t)s_min;
-            p.rec[2 * rid + 1] = ((unsigned long long)s_off << 32) | (uint32_t)s_size;
+            p.rec[3 * rid] = ((unsigned long long)(uint32_t)cls << 32) | (uint32_t)s_min;
+            p.rec[3 * rid + 1] = ((unsigned long long)s_off << 32) | (uint32_t)s_size;
+            p.rec[3 * rid + 2] = (uint32_t)(ex == 0 ? v : u);   // the endpoint left in the remainder
             atomicAdd(p.cnt + cls, 1);
         }
     }
@@ -233,6 +255,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
     long long bytes = 0;
     __shared__ int s_task;
 
+    phase_mark(&p.ctr->phase_ns[0]);
     if (!p.full) {
         // ---- P0: unions of inserted edges ---------------------------------------------------
         for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
@@ -267,38 +290,124 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
                 p.uf[l] = l;
             }
         }
-        // ---- P1: one block per deletion -----------------------------------------------------
+        phase_mark(&p.ctr->phase_ns[1]);
+        // ---- P1a: one warp per deletion: a common neighbour settles it (most deletions in a
+        // dense component, hub-hub ones included); the rest go to the hard list -------------
+        for (int64_t b = (int64_t)wid * WARP; b < nh; b += (int64_t)W * WARP) {
+            // 32 half-edits per warp iteration, then each candidate checked by the whole warp
+            int64_t k0 = b + lane_id();
+            bool cand = false;
+            int32_t x = 0, y = 0;
+            if (k0 < nh) {
+                unsigned long long key = p.hkeys[k0];
+                x = (int32_t)(key >> (p.B + 1));
+                y = (int32_t)(key & ((1ull << p.B) - 1));
+                cand = ((key >> p.B) & 1ull) == 1ull && x < y && ld_volatile(p.label + x) == ld_volatile(p.label + y);
+            }
+            unsigned cm = __ballot_sync(0xffffffffu, cand);
+            while (cm) {
+                const int l = __ffs(cm) - 1;
+                cm &= cm - 1;
+                const int32_t cx = __shfl_sync(0xffffffffu, x, l), cy = __shfl_sync(0xffffffffu, y, l);
+                Row ra = p.g.row[cx], rb = p.g.row[cy];
+                if (rb.len < ra.len) { Row tmp = ra; ra = rb; rb = tmp; }
+                const int32_t* av = p.g.pool + ra.start;
+                const int32_t* bv = p.g.pool + rb.start;
+                bool met = false;
+                for (int i0 = 0; i0 < ra.len && !met; i0 += WARP) {
+                    int i = i0 + (int)lane_id();
+                    bool h = false;
+                    if (i < ra.len) {
+                        long long kk = lower_bound_i32(bv, rb.len, av[i]);
+                        h = kk < rb.len && bv[kk] == av[i];
+                    }
+                    met = __any_sync(0xffffffffu, h);
+                    if (i < ra.len) bytes += 4LL * 8;
+                }
+                if (lane_id() == 0) {
+                    atomicAdd(&p.ctr->searches, 1);
+                    if (!met) {
+                        // a class with more deletions to search than the limit is recomputed
+                        // instead; every unsettled deletion is listed so P1b can reset hcnt
+                        const int32_t cls = ld_volatile(p.label + cx);
+                        const int before = atomicAdd(p.hcnt + cls, 1);
+                        const int at = atomicAdd(&p.ctr->list_count[0], 1);
+                        if (at < p.hard_cap) p.hard[at] = (int32_t)(b + l);
+                        const bool over = at >= p.hard_cap || (p.search_limit >= 0 && before >= p.search_limit);
+                        if (over && atomicExch(p.dirty + cls, p.epoch) != p.epoch)
+                            atomicAdd(&p.ctr->recomputes, 1);
+                    }
+                }
+            }
+        }
+        if (!grid_sync(p.bar, 39)) return;
+        phase_mark(&p.ctr->phase_ns[2]);
+        // ---- P1b: one block per remaining deletion: the bounded bidirectional search ---------
+        const int nhard = min(ld_volatile(&p.ctr->list_count[0]), p.hard_cap);
+        if (leader) p.ctr->noop = ld_volatile(&p.ctr->searches) - nhard;   // settled by a common neighbour
         while (true) {
-            if (threadIdx.x == 0) s_task = atomicAdd(&p.ctr->list_count[3], 1);
+            if (threadIdx.x == 0) {
+                int j = atomicAdd(&p.ctr->list_count[3], 1);
+                if (j < nhard) {
+                    // the class of a listed deletion is fixed since P0; a dirty one is not searched
+                    unsigned long long key = p.hkeys[p.hard[j]];
+                    int32_t cls = ld_volatile(p.label + (int32_t)(key >> (p.B + 1)));
+                    p.hcnt[cls] = 0;
+                    if (ld_volatile(p.dirty + cls) == p.epoch) j = -1;
+                }
+                s_task = j;
+            }
             __syncthreads();
-            const int k = s_task;
+            const int j = s_task;
             __syncthreads();
-            if (k >= nh) break;
-            unsigned long long key = p.hkeys[k];
-            int op = (int)((key >> p.B) & 1ull);
+            if (j >= nhard) break;
+            if (j < 0) continue;
+            unsigned long long key = p.hkeys[p.hard[j]];
             int32_t x = (int32_t)(key >> (p.B + 1));
             int32_t y = (int32_t)(key & ((1ull << p.B) - 1));
-            if (op != 1 || x > y) continue;
             int32_t cls = ld_volatile(p.label + x);
-            if (cls != ld_volatile(p.label + y)) continue;
-            if (threadIdx.x == 0) atomicAdd(&p.ctr->searches, 1);
-            int res = cc_search(p, x, y, cls, bytes);
+            int res = cc_search(p, x, y, cls, bytes, true);
             if (threadIdx.x == 0 && res == 2 && atomicExch(p.dirty + cls, p.epoch) != p.epoch)
                 atomicAdd(&p.ctr->recomputes, 1);
             __syncthreads();
         }
         if (!grid_sync(p.bar, 32)) return;
-        // ---- P2: single splits relabel locally; the rest are dirty ----------------------------
-        const int nrec = min(ld_volatile(&p.ctr->list_count[2]), (int)(p.rec_cap / 2));
+        phase_mark(&p.ctr->phase_ns[3]);
+        // ---- P2: relabel the split sides -------------------------------------------------------
+        // A class whose deletions all ended connected or split is exact once its remainder R
+        // (the class minus the split sides) is known to be connected. Every component of R
+        // holds the surviving endpoint of some split deletion, so R is connected iff those
+        // endpoints are: trivially with one split; with several, each endpoint is searched
+        // against the class's first one. Any other outcome marks the class dirty.
+        const int nrec = min(ld_volatile(&p.ctr->list_count[2]), (int)(p.rec_cap / 3));
+        for (int i = (int)tid; i < nrec; i += (int)T) {
+            int32_t cls = (int32_t)(p.rec[3 * i] >> 32);
+            if (ld_volatile(p.dirty + cls) != p.epoch && ld_volatile(p.cnt + cls) >= 2)
+                atomicCAS(p.firstw + cls, -1, (int32_t)p.rec[3 * i + 2]);
+        }
+        if (!grid_sync(p.bar, 40)) return;
+        while (true) {
+            if (threadIdx.x == 0) s_task = atomicAdd(&p.ctr->q_count[0], 1);
+            __syncthreads();
+            const int i = s_task;
+            __syncthreads();
+            if (i >= nrec) break;
+            int32_t cls = (int32_t)(p.rec[3 * i] >> 32);
+            if (ld_volatile(p.cnt + cls) < 2 || ld_volatile(p.dirty + cls) == p.epoch) continue;
+            int32_t w = (int32_t)p.rec[3 * i + 2], f = ld_volatile(p.firstw + cls);
+            if (w == f || f < 0) continue;
+            int res = cc_search(p, w, f, cls, bytes, false);
+            if (threadIdx.x == 0 && res != 0 && atomicExch(p.dirty + cls, p.epoch) != p.epoch)
+                atomicAdd(&p.ctr->recomputes, 1);
+            __syncthreads();
+        }
+        if (!grid_sync(p.bar, 41)) return;
         for (int i = wid; i < nrec; i += W) {
-            unsigned long long r0 = p.rec[2 * i], r1 = p.rec[2 * i + 1];
+            unsigned long long r0 = p.rec[3 * i], r1 = p.rec[3 * i + 1];
             int32_t cls = (int32_t)(r0 >> 32), mn = (int32_t)(r0 & 0xffffffffu);
             long long off = (long long)(r1 >> 32);
             int size = (int)(r1 & 0xffffffffu);
-            if (ld_volatile(p.dirty + cls) == p.epoch || ld_volatile(p.cnt + cls) != 1) {
-                if (lane_id() == 0 && atomicExch(p.dirty + cls, p.epoch) != p.epoch) atomicAdd(&p.ctr->recomputes, 1);
-                continue;
-            }
+            if (ld_volatile(p.dirty + cls) == p.epoch) continue;
             if (lane_id() == 0) {
                 atomicAdd(&p.ctr->splits, 1);
                 if (mn == cls) p.remf[cls] = p.epoch;
@@ -341,9 +450,10 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
         if (!grid_sync(p.bar, 35)) return;
         // restore per-class scratch of split classes
         for (int i = (int)tid; i < nrec; i += (int)T) {
-            int32_t cls = (int32_t)(p.rec[2 * i] >> 32);
+            int32_t cls = (int32_t)(p.rec[3 * i] >> 32);
             p.cnt[cls] = 0;
             p.newmin[cls] = INT32_MAX;
+            p.firstw[cls] = -1;
         }
     } else {
         for (int64_t v = tid; v < n; v += T) {
@@ -363,38 +473,103 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
         p.vp[v] = d ? (int32_t)v : -1;
     }
     if (!grid_sync(p.bar, 36)) return;
-    for (int v = wid; v < n; v += W) {   // rows up to CC_BIG: one warp each
-        if (ld_volatile(p.vp + v) < 0) continue;
-        Row r = p.g.row[v];
-        if (r.len > CC_BIG) continue;
-        const int32_t* rw = p.g.pool + r.start;
-        for (int b0 = 0; b0 < r.len; b0 += WARP) {
-            int k = b0 + (int)lane_id();
-            if (k < r.len) {
-                int32_t w = rw[k];
-                if (w > v) {
-                    // an edge leaving a dirty class means the uploaded labels did not describe
-                    // the components of the graph; flagged instead of followed
+    {
+        // Afforest (Sutton, Ben-Nun, Barak, IPDPS 2018): link every dirty vertex to its first
+        // two neighbours, compress, estimate the dominant root by sampling, then only vertices
+        // outside that root scan the rest of their rows (an edge between the dominant tree
+        // and another vertex is linked from the other vertex's row). An edge leaving a dirty
+        // class means the uploaded labels did not describe the components of the graph: it is
+        // flagged (SCOUT_E_STATE) instead of followed.
+        constexpr int AF_FIRST = 2;
+        for (int r = 0; r < AF_FIRST; r++) {
+            for (int64_t v = tid; v < n; v += T) {
+                if (ld_volatile(p.vp + v) < 0) continue;
+                Row rr = p.g.row[v];
+                if (r < rr.len) {
+                    int32_t w = p.g.pool[rr.start + r];
+                    if (ld_volatile(p.vp + w) < 0) atomicExch(&p.ctr->pad, 1);
+                    else uf_union(p.vp, (int32_t)v, w);
+                }
+            }
+            if (!grid_sync(p.bar, 42 + r)) return;
+        }
+        for (int64_t v = tid; v < n; v += T)
+            if (ld_volatile(p.vp + v) >= 0) p.vp[v] = uf_find(p.vp, (int32_t)v);
+        if (tid == 0) bytes += 24LL * n;
+        if (!grid_sync(p.bar, 44)) return;
+        if (blockIdx.x == 0) {   // mode of the roots of up to 1024 sampled dirty vertices
+            __shared__ int32_t s_key[2048];
+            __shared__ int s_cnt[2048];
+            __shared__ unsigned long long s_best;
+            for (int i = threadIdx.x; i < 2048; i += CC_THREADS) { s_key[i] = -1; s_cnt[i] = 0; }
+            if (threadIdx.x == 0) s_best = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < 4096; i += CC_THREADS) {
+                int64_t v = (int64_t)(((unsigned long long)i * 2654435761ull) % (unsigned long long)n);
+                int32_t r = ld_volatile(p.vp + v);
+                if (r < 0) continue;
+                unsigned h = ((unsigned)r * 2654435761u) & 2047u;
+                for (int pr = 0; pr < 2048; pr++) {
+                    int32_t prev = atomicCAS(&s_key[h], -1, r);
+                    if (prev == -1 || prev == r) { atomicAdd(&s_cnt[h], 1); break; }
+                    h = (h + 1) & 2047u;
+                }
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < 2048; i += CC_THREADS)
+                if (s_cnt[i] > 0)
+                    atomicMax(&s_best, ((unsigned long long)s_cnt[i] << 32) | (uint32_t)s_key[i]);
+            __syncthreads();
+            if (threadIdx.x == 0) p.ctr->aux64[1] = s_best ? (long long)(uint32_t)(s_best & 0xffffffffu) : -1;
+        }
+        if (!grid_sync(p.bar, 45)) return;
+        const int32_t gr = (int32_t)ld_volatile(&p.ctr->aux64[1]);
+        // compact lists of the vertices outside the dominant root (short rows / long rows)
+        if (leader) { p.ctr->q_count[1] = 0; p.ctr->q_count[2] = 0; }
+        if (!grid_sync(p.bar, 46)) return;
+        for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
+            int64_t v = b + lane_id();
+            bool sm_ = false, bg = false;
+            if (v < n) {
+                int32_t pv = ld_volatile(p.vp + v);
+                if (pv >= 0 && pv != gr) {
+                    int len = p.g.row[v].len;
+                    if (len > AF_FIRST) { bg = len > CC_BIG; sm_ = !bg; }
+                }
+            }
+            int a = warp_append(sm_, &p.ctr->q_count[1]);
+            if (sm_) p.merged[a] = (int32_t)v;
+            int c2 = warp_append(bg, &p.ctr->q_count[2]);
+            if (bg) p.side[c2] = (int32_t)v;
+        }
+        if (tid == 0) bytes += 8LL * n;
+        if (!grid_sync(p.bar, 47)) return;
+        const int nsmall = ld_volatile(&p.ctr->q_count[1]), nbig = ld_volatile(&p.ctr->q_count[2]);
+        for (int i = wid; i < nsmall; i += W) {   // rows up to CC_BIG: one warp each
+            const int32_t v = p.merged[i];
+            Row r = p.g.row[v];
+            const int32_t* rw = p.g.pool + r.start;
+            for (int b0 = AF_FIRST; b0 < r.len; b0 += WARP) {
+                int k = b0 + (int)lane_id();
+                if (k < r.len) {
+                    int32_t w = rw[k];
                     if (ld_volatile(p.vp + w) < 0) atomicExch(&p.ctr->pad, 1);
                     else uf_union(p.vp, v, w);
                 }
             }
+            if (lane_id() == 0) bytes += 8LL * r.len;
         }
-        if (lane_id() == 0) bytes += 8LL * r.len;
-    }
-    for (int v = blockIdx.x; v < n; v += gridDim.x) {   // longer rows: one block each
-        if (ld_volatile(p.vp + v) < 0) continue;
-        Row r = p.g.row[v];
-        if (r.len <= CC_BIG) continue;
-        const int32_t* rw = p.g.pool + r.start;
-        for (long long k = threadIdx.x; k < r.len; k += CC_THREADS) {
-            int32_t w = rw[k];
-            if (w > v) {
+        for (int i = blockIdx.x; i < nbig; i += gridDim.x) {   // longer rows: one block each
+            const int32_t v = p.side[i];
+            Row r = p.g.row[v];
+            const int32_t* rw = p.g.pool + r.start;
+            for (long long k = AF_FIRST + threadIdx.x; k < r.len; k += CC_THREADS) {
+                int32_t w = rw[k];
                 if (ld_volatile(p.vp + w) < 0) atomicExch(&p.ctr->pad, 1);
                 else uf_union(p.vp, v, w);
             }
+            if (threadIdx.x == 0) bytes += 8LL * r.len;
         }
-        if (threadIdx.x == 0) bytes += 8LL * r.len;
     }
     if (!grid_sync(p.bar, 37)) return;
     for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
@@ -408,35 +583,34 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
     }
     if (tid == 0) bytes += 16LL * n;
 done:
+    phase_mark(&p.ctr->phase_ns[4]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
     if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
     if (leader) p.ctr->affected = p.ctr->changed;
 }
 
-__global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, int32_t* __restrict__ newmin, int64_t n) {
+__global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, int32_t* __restrict__ newmin,
+                          int32_t* __restrict__ firstw, int64_t n) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         uf[v] = (int32_t)v;
         cnt[v] = 0;
         newmin[v] = INT32_MAX;
+        firstw[v] = -1;
     }
 }
 
 static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
     SCOUT_RC(lists_ensure(c));
     const int64_t n = c->n;
-    if (!c->d_misc || c->cap_misc < 6 * n) {   // uf, cnt, dirty, remf, newmin, vp
-        if (c->d_misc) dev_free(c, c->d_misc, (size_t)c->cap_misc * 4);
-        c->d_misc = nullptr;
-        c->cap_misc = 0;
-        SCOUT_RC(dev_alloc(c, &c->d_misc, (size_t)6 * n * 4, "component scratch"));
-        c->cap_misc = 6 * n;
-        SCOUT_CU(c, cudaMemsetAsync(c->d_misc, 0, (size_t)6 * n * 4, c->s_main));
-        int32_t* base = (int32_t*)c->d_misc;
-        k_cc_init<<<blocks_for(n, 256), 256, 0, c->s_main>>>(base, base + n, base + 4 * n, n);
+    if (!c->d_cc) {   // uf, cnt, dirty, remf, newmin, vp, firstw, hcnt
+        SCOUT_RC(dev_alloc(c, (void**)&c->d_cc, (size_t)8 * n * 4, "component scratch"));
+        SCOUT_CU(c, cudaMemsetAsync(c->d_cc, 0, (size_t)8 * n * 4, c->s_main));
+        int32_t* base = c->d_cc;
+        k_cc_init<<<blocks_for(n, 256), 256, 0, c->s_main>>>(base, base + n, base + 4 * n, base + 6 * n, n);
         SCOUT_LAUNCH(c, "k_cc_init");
     }
-    int32_t* base = (int32_t*)c->d_misc;
+    int32_t* base = c->d_cc;
     CcParams p;
     p.g = dgraph(c);
     p.label = c->label;
@@ -448,6 +622,13 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
     p.remf = base + 3 * n;
     p.newmin = base + 4 * n;
     p.vp = base + 5 * n;
+    p.firstw = base + 6 * n;
+    p.hcnt = base + 7 * n;
+    // the matched-deletion prefix of the merge (2 * ws_m int64) is free during the repair
+    p.hard = (int32_t*)c->d_mdp;
+    p.hard_cap = (int)std::min<int64_t>(4 * c->ws_m, INT32_MAX);   // > deletions, so never full
+    int64_t limit = sched && sched->search_limit != 0 ? sched->search_limit : 32;
+    p.search_limit = (int)std::max<int64_t>(-1, std::min<int64_t>(limit, INT32_MAX));
     p.merged = c->d_list[1];
     p.rec = (unsigned long long*)c->d_qbuf[0];
     p.rec_cap = c->qcap;

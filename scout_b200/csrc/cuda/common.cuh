@@ -143,6 +143,11 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, int tag = 0) {
 
 __device__ __forceinline__ void grid_fail(GridBar* b, int code) { atomicCAS(&b->err, 0, code); }
 
+// Phase timestamp written by one thread right after a grid barrier (profiling aid).
+__device__ __forceinline__ void phase_mark(unsigned long long* slot) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *slot = globaltimer_ns();
+}
+
 // Global warp index / count for grid-stride warp loops.
 __device__ __forceinline__ int gwarp_id() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) / WARP); }
 __device__ __forceinline__ int gwarp_count() { return (int)((gridDim.x * blockDim.x) / WARP); }

@@ -37,6 +37,7 @@ struct DevCounters {
     int pad;
     long long hbm_bytes;      // algorithmic bytes of the repair
     long long aux64[4];
+    unsigned long long phase_ns[8];   // %globaltimer marks written by the repair kernels
 };
 
 struct scout_ctx {
@@ -108,7 +109,8 @@ struct scout_ctx {
     uint32_t qtag = 1;                               // per-round dedupe tags, never reused
     unsigned int* d_sort_hist = nullptr; int64_t cap_hist = 0;
     int64_t* d_scan_tmp = nullptr;  int64_t cap_scan = 0;
-    void* d_misc = nullptr;         int64_t cap_misc = 0;   // kernel-specific scratch
+    void* d_misc = nullptr;         int64_t cap_misc = 0;   // colouring proposal markers
+    int32_t* d_cc = nullptr;        // component scratch (7 n int32)
 
     DevCounters* d_ctr = nullptr;
     DevCounters* h_ctr = nullptr;   // pinned
