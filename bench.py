@@ -13,8 +13,8 @@ deletions of existing edges and half insertions of non-edges. Seeded synthetic d
 value  edge-updates/s with the edits already in HBM: classification + merge into the rows +
        repair, from the library's CUDA events on its own stream.
 e2e    the same through the public C ABI with host buffers: each step copies the edits from
-       host memory, repairs and copies the changed solution entries back into a host mirror
-       (scout_repair + scout_commit), timed with CUDA events around the step loop.
+       page-locked host memory, repairs and copies the changed solution entries back into a
+       host mirror (scout_repair + scout_commit), timed with CUDA events around the step loop.
 Multi-GPU (torchrun): every rank runs an independent replica stream (no collective on the
 data path), value = all ranks' updates / max over ranks of the elapsed time.
 """
@@ -48,12 +48,13 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="scout", choices=["scout", "reference"])
     ap.add_argument("--scale", type=int, default=22)
-    ap.add_argument("--problems", default="bfs")
+    ap.add_argument("--problems", default="bfs,coloring")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-sample", type=int, default=20000, help="edits per batch timed in the reference arm")
     ap.add_argument("--ref-timeout", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--verbose", action="store_true", help="per-batch statistics on stderr")
     return ap.parse_args()
 
 
@@ -181,7 +182,7 @@ def measured_peak():
 # ---------------------------------------------------------------------------------------
 # scout arm
 # ---------------------------------------------------------------------------------------
-def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, clocks):
+def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, clocks, verbose=False):
     import torch
 
     import scout_b200 as sb
@@ -189,6 +190,8 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
     ctx.load_csr(off, adj)
     ctx.upload(problem, init)
     mirror = init.copy()
+    # each step's edits are read from page-locked host memory (copied there before timing)
+    batches = [sb.pinned_copy(b) for b in batches[:warmup + steps]]
     for b in batches[:warmup]:
         ctx.repair(problem, b)
         ctx.commit(problem, mirror)
@@ -218,28 +221,40 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
     for st in per:
         e0, e1 = st.pop("_ev")
         st["ms_step"] = e0.elapsed_time(e1)
+        if verbose:
+            keep = ("edits", "ms_step", "ms_h2d", "ms_update", "ms_repair", "rounds", "changed", "launches")
+            d = {k: (round(st[k], 3) if isinstance(st[k], float) else st[k]) for k in keep}
+            d["phase_ms"] = [round(x, 3) for x in st["phase_ms"]]
+            print(problem, json.dumps(d), file=sys.stderr, flush=True)
     ctx.close()
     return per, e2e_ms
 
 
-def cpu_baseline(problem, off, adj, init, batches, seconds):
-    """The oracle (single-thread CPU restatement of the reference engine) on a bounded sample."""
+def cpu_baseline(problems, off, adj, init, batches, seconds):
+    """The oracle (single-thread CPU restatement of the reference engine) on a bounded sample:
+    the same stream's batches in order, about seconds / len(problems) per problem."""
     from oracle import oracle as orc
-    eng = orc.Engine(problem, off, adj, init)
     edits = 0
     t_used = 0.0
-    k = 0
-    for b in batches:
-        if t_used >= seconds:
-            break
-        t0 = time.perf_counter()
-        eng.batch(b)
-        t_used += time.perf_counter() - t0
-        edits += len(b)
-        k += 1
+    parts = []
+    for p in problems:
+        eng = orc.Engine(p, off, adj, init[p])
+        t_p = 0.0
+        k = e_p = 0
+        for b in batches:
+            if t_p >= seconds / len(problems):
+                break
+            t0 = time.perf_counter()
+            eng.batch(b)
+            t_p += time.perf_counter() - t0
+            e_p += len(b)
+            k += 1
+        parts.append(f"{p}: first {k} batches ({e_p} toggles) in {t_p:.1f} s")
+        edits += e_p
+        t_used += t_p
     return {"value": edits / t_used if t_used else None, "unit": "edge-updates/s", "cores": 1, "kind": "port",
-            "sample": f"{problem}: first {k} batches ({edits} toggles) of the same stream, oracle restatement "
-                      f"of the reference engine, {t_used:.1f} s single-threaded"}
+            "sample": "oracle restatement of the reference engine, single-threaded, on the same stream; "
+                      + "; ".join(parts)}
 
 
 def scout_arm(a, dist):
@@ -251,7 +266,7 @@ def scout_arm(a, dist):
     results = {}
     clocks = Clocks(device)
     for p in problems:
-        results[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks)
+        results[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks, a.verbose)
     clk = clocks.summary()
     peak, peak_kind = measured_peak()
     per_problem = {}
@@ -315,8 +330,7 @@ def scout_arm(a, dist):
         "gpu_launches": int(launches), "clocks": clk,
     }
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
-        p0 = problems[0]
-        line["cpu_baseline"] = cpu_baseline(p0, off, adj, init[p0], batches, a.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(problems, off, adj, init, batches, a.cpu_seconds)
     return line
 
 
@@ -337,7 +351,7 @@ def reference_arm(a, dist):
     cores = os.cpu_count()
     if not have:
         # the oracle port of the reference engine on the host cores (single thread)
-        cb = cpu_baseline(problems[0], off, adj, init[problems[0]], sample, a.cpu_seconds * 2)
+        cb = cpu_baseline(problems, off, adj, init, sample, a.cpu_seconds * 2)
         return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "edge-updates/s",
                 "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "edge-updates/s", "h2d_bytes_per_step": 0,

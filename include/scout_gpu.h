@@ -178,6 +178,13 @@ int scout_recompute_cc(scout_ctx* ctx, scout_batch_stats* stats);
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 
+/* Page-locked host memory for edit batches and mirrors (alloc_pair's pinned half,
+ * core/gpu_common.h:43-52). Edits passed to scout_repair from such memory are copied to the
+ * device directly; edits in pageable memory go through the context's pinned staging buffer
+ * first. */
+int scout_host_alloc(uint64_t bytes, void** out);
+int scout_host_free(void* p);
+
 /* ---- allocation-free entry point ------------------------------------------------------ */
 /* No counterpart in the reference. BFS levels from `source` (-1 unreached) over a CSR that
  * the caller already holds in device memory (d_off: n + 1 int64 offsets, d_adj: int32

@@ -83,6 +83,8 @@ SIGNATURES = [
     ("scout_recompute_bfs", C.c_int, [_vp, C.c_int32, C.POINTER(ScoutBatchStats)]),
     ("scout_recompute_cc", C.c_int, [_vp, C.POINTER(ScoutBatchStats)]),
     ("scout_sync", C.c_int, [_vp, C.c_int64]),
+    ("scout_host_alloc", C.c_int, [C.c_uint64, C.POINTER(_vp)]),
+    ("scout_host_free", C.c_int, [_vp]),
     ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h
     ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),

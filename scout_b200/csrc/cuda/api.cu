@@ -69,9 +69,9 @@ static void release(scout_ctx* c) {
     cudaSetDevice(c->device);
     if (c->s_main) cudaStreamSynchronize(c->s_main);
     for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
-    void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c,
+    void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c, c->stamp_d,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
-                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_misc, c->d_cc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
+                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
                     c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
     for (void* p : devs) if (p) cudaFree(p);
     void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
@@ -400,6 +400,28 @@ int scout_sync(scout_ctx* c, int64_t timeout_us) {
                 return c->fail(SCOUT_E_TIMEOUT, "scout_sync timed out");
             std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
+    }
+    return SCOUT_OK;
+}
+
+int scout_host_alloc(uint64_t bytes, void** out) {
+    if (!out) return host_fail(SCOUT_E_INVALID, "scout_host_alloc: null output");
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, (size_t)std::max<uint64_t>(bytes, 1), cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return host_fail(SCOUT_E_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    }
+    return SCOUT_OK;
+}
+
+int scout_host_free(void* p) {
+    if (!p) return SCOUT_OK;
+    cudaError_t e = cudaFreeHost(p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return host_fail(SCOUT_E_CUDA, std::string("cudaFreeHost: ") + cudaGetErrorString(e));
     }
     return SCOUT_OK;
 }

@@ -34,6 +34,7 @@ struct BfsParams {
     int32_t* st_inval;
     int32_t* st_touch;
     uint32_t* st_q;
+    int32_t* found;     // == tag: a chunk of a long candidate found a valid parent this round
     int32_t epoch;
     uint32_t qtag0;
     DevCounters* ctr;
@@ -60,7 +61,7 @@ __device__ __forceinline__ void push_vertex(const BfsParams& p, bool pred, int32
     if (first) {
         if (chunked) {
             int len = p.g.row[y].len;
-            nit = (len + CHUNK - 1) / CHUNK;
+            nit = max(1, (len + CHUNK - 1) / CHUNK);   // an empty row still gets its item
         } else {
             nit = 1;
         }
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
     int rounds = 0;
     uint32_t tag = p.qtag0;
     int cur = 0;
+    phase_mark(&p.ctr->phase_ns[0]);
 
     if (p.mode == 1) {
         // Full recompute: every vertex restarts at +inf; all become touched.
@@ -163,6 +165,11 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
         if (!grid_sync(p.bar, 1)) return;
     } else {
         // ---- A: invalidation -------------------------------------------------------------
+        // Candidates are queued as CHUNK-sized items of their rows. A single-chunk candidate
+        // is settled by one warp (parent check, invalidation, children pushed). A longer one
+        // is checked chunk by chunk (any chunk with a valid parent marks found = tag); after
+        // a barrier its first item decides, and after another every chunk of an invalidated
+        // candidate pushes its children, so a hub's row is spread over many warps.
         const int nh = ld_volatile(&p.ctr->n_half);
         tag++;
         for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
@@ -179,7 +186,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     cand = lx >= 0 && ly == lx + 1;
                 }
             }
-            push_vertex(p, cand, y, 0, tag, false, false);
+            push_vertex(p, cand, y, 0, tag, true, false);
         }
         if (!grid_sync(p.bar, 2)) return;
         cur = 0;
@@ -190,21 +197,36 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
             if (leader) p.ctr->q_count[zer] = 0;
             tag++;
             for (int i = wid; i < cnt; i += W) {
-                int32_t c = (int32_t)(p.q[cur][i] & 0xffffffffu);
-                int lc = ld_level(p.level + c);
-                if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) continue;
-                Row r = p.g.row[c];
-                const int32_t* rw = p.g.pool + r.start;
+                const unsigned long long item = p.q[cur][i];
+                const int32_t c = (int32_t)(item & 0xffffffffu);
+                const int chunk = (int)(item >> 32);
+                const Row r = p.g.row[c];
+                const bool big = r.len > CHUNK;
+                const int lc = ld_level(p.level + c);
+                if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) {
+                    if (big && lane_id() == 0) p.found[c] = (int32_t)tag;   // nothing to decide
+                    continue;
+                }
+                const long long c0 = (long long)chunk * CHUNK;
+                const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+                const int32_t* rw = p.g.pool + r.start + c0;
                 bool found = false;
-                for (int b0 = 0; b0 < r.len && !found; b0 += WARP) {
+                for (int b0 = 0; b0 < clen && !found; b0 += WARP) {
                     int k = b0 + (int)lane_id();
                     bool ok = false;
-                    if (k < r.len) {
+                    if (k < clen) {
                         int32_t w = rw[k];
                         ok = ld_level(p.level + w) == lc - 1 && ld_volatile(p.st_inval + w) != p.epoch;
                     }
                     found = __any_sync(0xffffffffu, ok);
-                    if (k < r.len) bytes += 8;
+                    if (k < clen) bytes += 8;
+                }
+                if (big) {
+                    if (lane_id() == 0) {
+                        if (found) p.found[c] = (int32_t)tag;
+                        if (chunk == 0) p.ctr->list_count[2] = 1;   // a long candidate this round
+                    }
+                    continue;
                 }
                 if (found) continue;
                 if (lane_id() == 0) {
@@ -213,24 +235,73 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     p.inval[at] = c;
                 }
                 __syncwarp();
-                for (int b0 = 0; b0 < r.len; b0 += WARP) {
+                for (int b0 = 0; b0 < clen; b0 += WARP) {
                     int k = b0 + (int)lane_id();
                     bool ch = false;
                     int32_t w = 0;
-                    if (k < r.len) {
+                    if (k < clen) {
                         w = rw[k];
                         ch = ld_level(p.level + w) == lc + 1 && ld_volatile(p.st_inval + w) != p.epoch;
                     }
-                    push_vertex(p, ch, w, nxt, tag, false, false);
+                    push_vertex(p, ch, w, nxt, tag, true, false);
                 }
-                if (lane_id() == 0) bytes += 8LL * r.len + 24;
+                if (lane_id() == 0) bytes += 8LL * clen + 24;
+            }
+            if (!grid_sync(p.bar, 3)) return;
+            if (ld_volatile(&p.ctr->list_count[2])) {
+                // long candidates: decide on the first item, then push children from every chunk
+                for (int64_t b = tid - (tid & (WARP - 1)); b < cnt; b += T) {
+                    const int64_t i = b + lane_id();
+                    bool nt = false;
+                    int32_t c = 0;
+                    if (i < cnt) {
+                        const unsigned long long item = p.q[cur][i];
+                        c = (int32_t)(item & 0xffffffffu);
+                        if ((item >> 32) == 0 && p.g.row[c].len > CHUNK && ld_volatile(p.found + c) != (int32_t)tag)
+                            nt = atomicExch(&p.st_inval[c], p.epoch) != p.epoch;
+                    }
+                    int at = warp_append(nt, &p.ctr->list_count[0]);
+                    if (nt) p.inval[at] = c;
+                }
+                if (!grid_sync(p.bar, 8)) return;
+                if (leader) p.ctr->list_count[2] = 0;
+                for (int i = wid; i < cnt; i += W) {
+                    const unsigned long long item = p.q[cur][i];
+                    const int32_t c = (int32_t)(item & 0xffffffffu);
+                    const Row r = p.g.row[c];
+                    if (r.len <= CHUNK || ld_volatile(p.found + c) == (int32_t)tag ||
+                        ld_volatile(p.st_inval + c) != p.epoch)
+                        continue;
+                    const int lc = ld_level(p.level + c);
+                    const long long c0 = (long long)(item >> 32) * CHUNK;
+                    const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+                    const int32_t* rw = p.g.pool + r.start + c0;
+                    for (int b0 = 0; b0 < clen; b0 += WARP) {
+                        int k = b0 + (int)lane_id();
+                        bool ch = false;
+                        int32_t w = 0;
+                        if (k < clen) {
+                            w = rw[k];
+                            ch = ld_level(p.level + w) == lc + 1 && ld_volatile(p.st_inval + w) != p.epoch;
+                        }
+                        push_vertex(p, ch, w, nxt, tag, true, false);
+                    }
+                    if (lane_id() == 0) bytes += 8LL * clen;
+                }
+                if (!grid_sync(p.bar, 9)) return;
             }
             rounds++;
-            if (!grid_sync(p.bar, 3)) return;
             cur = nxt;
         }
+        phase_mark(&p.ctr->phase_ns[1]);
         // ---- B: reset and seed --------------------------------------------------------------
+        // Every invalidated vertex restarts at +inf and queues its row's chunks in q[2]; each
+        // chunk then offers (min level of its valid neighbours) + 1. Inserted edges seed their
+        // endpoints. Both push into q[0], where the relax rounds start.
+        if (leader) { p.ctr->q_count[0] = 0; p.ctr->q_count[1] = 0; p.ctr->q_count[2] = 0; }
+        if (!grid_sync(p.bar, 4)) return;
         const int ninv = ld_volatile(&p.ctr->list_count[0]);
+        tag++;
         for (int64_t b = tid - (tid & (WARP - 1)); b < ninv; b += T) {
             int64_t i = b + lane_id();
             bool ok = i < ninv;
@@ -242,21 +313,23 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
             }
             int ti = warp_append(nt, &p.ctr->changed);
             if (nt) p.touched[ti] = c;
+            push_vertex(p, ok, c, 2, tag, true, false);
         }
-        // all queues restart empty for phase C
-        if (!grid_sync(p.bar, 4)) return;
-        if (leader) { p.ctr->q_count[0] = 0; p.ctr->q_count[1] = 0; p.ctr->q_count[2] = 0; }
         if (!grid_sync(p.bar, 5)) return;
         tag++;
-        // boundary seeds: warp per invalidated vertex
-        for (int i = wid; i < ninv; i += W) {
-            int32_t c = p.inval[i];
-            Row r = p.g.row[c];
-            const int32_t* rw = p.g.pool + r.start;
+        // boundary seeds: warp per chunk of an invalidated vertex's row
+        const int nseed = qcount(p, 2);
+        for (int i = wid; i < nseed; i += W) {
+            const unsigned long long item = p.q[2][i];
+            const int32_t c = (int32_t)(item & 0xffffffffu);
+            const Row r = p.g.row[c];
+            const long long c0 = (long long)(item >> 32) * CHUNK;
+            const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+            const int32_t* rw = p.g.pool + r.start + c0;
             unsigned best = 0xffffffffu;
-            for (int b0 = 0; b0 < r.len; b0 += WARP) {
+            for (int b0 = 0; b0 < clen; b0 += WARP) {
                 int k = b0 + (int)lane_id();
-                if (k < r.len) {
+                if (k < clen) {
                     int32_t w = rw[k];
                     if (ld_volatile(p.st_inval + w) != p.epoch) {
                         int lw = ld_level(p.level + w);
@@ -266,7 +339,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-            if (lane_id() == 0) bytes += 8LL * r.len + 24;
+            if (lane_id() == 0) bytes += 8LL * max(clen, 0) + 24;
             bool dec = false;
             if (lane_id() == 0 && best != 0xffffffffu) {
                 unsigned cand = best + 1;
@@ -299,6 +372,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
         if (!grid_sync(p.bar, 6)) return;
         cur = 0;
     }
+    phase_mark(&p.ctr->phase_ns[2]);
     // ---- C: relax rounds -------------------------------------------------------------------
     while (true) {
         const int cnt = qcount(p, cur);
@@ -311,6 +385,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
         if (!grid_sync(p.bar, 7)) return;
         cur = nxt;
     }
+    phase_mark(&p.ctr->phase_ns[3]);
     // ---- counters ----------------------------------------------------------------------------
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
@@ -337,6 +412,7 @@ static int bfs_launch(scout_ctx* c, int mode, scout_batch_stats* st) {
     p.st_inval = c->stamp_a;
     p.st_touch = c->stamp_b;
     p.st_q = (uint32_t*)c->stamp_c;
+    p.found = c->stamp_d;
     p.epoch = (int32_t)c->epoch;
     p.qtag0 = c->qtag;
     p.ctr = c->d_ctr;

@@ -18,7 +18,8 @@ struct DevCounters {
     int n_del;          // edits classified as deletions
     int n_half;         // applied half-edits (2 per applied edit)
     int n_aff;          // vertices whose row changed
-    int n_small, n_large;
+    int n_small, n_large;     // rows planned by a warp / by a block
+    int n_slices, n_pad;      // merge slices
     long long new_elems;      // elements written to the pool this batch
     long long nnz_delta;      // inserted minus deleted entries
     long long update_bytes;   // algorithmic bytes of the row merge
@@ -79,6 +80,7 @@ struct scout_ctx {
     int32_t* stamp_a = nullptr;   // e.g. invalid / queued marks
     int32_t* stamp_b = nullptr;
     int32_t* stamp_c = nullptr;
+    int32_t* stamp_d = nullptr;
     int32_t* aux_v = nullptr;     // per-vertex int scratch (marker / uf parent)
     int32_t* aux_w = nullptr;
     uint32_t epoch = 0;
@@ -97,8 +99,11 @@ struct scout_ctx {
     int32_t* d_aff = nullptr;       // affected vertex ids (2m)
     int64_t* d_aff_seg = nullptr;   // [3 * 2m]: segment begin, first deletion, end
     int64_t* d_aff_len = nullptr;   // new length, then exclusive offsets (2m + 1)
-    int32_t* d_aff_small = nullptr; // (2m)
-    int32_t* d_aff_large = nullptr; // (2m)
+    int32_t* d_aff_small = nullptr; // rows planned by a warp (2m)
+    int32_t* d_aff_large = nullptr; // rows planned by a block (2m)
+    scout::Row* d_old_row = nullptr;   // descriptors of the affected rows before the batch (2m)
+    int64_t* d_slices = nullptr;  int64_t cap_slices = 0;   // merge items (row << 32 | slice)
+    int64_t* d_coff = nullptr;      // compaction offsets (n + 1)
     int key_bits = 0;
 
     // ---- per-vertex work lists (n-sized, allocated on first repair) ----
@@ -191,7 +196,7 @@ int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total);
 // graph.cu
 int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m, scout_batch_stats* st);
 int graph_ensure_scratch(scout_ctx* c);
-int graph_compact(scout_ctx* c, int64_t min_free);
+int graph_compact(scout_ctx* c, int64_t min_free, bool nnz_exact = false);
 int ws_ensure(scout_ctx* c, int64_t m);
 int lists_ensure(scout_ctx* c);
 int batch_begin(scout_ctx* c);   // zeroes the counters and the barrier for a new batch

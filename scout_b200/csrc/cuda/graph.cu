@@ -15,9 +15,12 @@
 //                     keys (u, op, v) and (v, op, u) per applied edit
 //   sort_keys         groups half-edits by vertex; inserts before deletes; neighbours sorted
 //   k_seg_heads/tails affected-vertex list and its key segments
-//   k_row_plan        per affected row: matched deletions (multiset cancel) -> new length
+//   k_row_alloc       old descriptor, new space (old length + insertions), planner, slices
 //   scan_i64          new rows' offsets in the pool
-//   k_merge_small/large  merge(old row minus deletions, insertions) into the new space
+//   k_row_plan_*      matched deletions (multiset cancel, tombstoned in the old row), new
+//                     length, insertions written to their final slots; warp or block per row
+//   k_merge_slices    survivors of the old row streamed into the new row, one warp per slice
+//                     of SLICE entries, so a hub row is spread over many warps
 #include "ctx.cuh"
 
 #include <algorithm>
@@ -25,8 +28,11 @@
 
 namespace scout {
 
-constexpr int SMALL_ROW_LIMIT = 2048;   // rows up to this size are merged by one warp
-constexpr int LARGE_THREADS = 512;
+constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the merge
+constexpr int HEAVY_EDITS = 64;      // rows with more half-edits are planned by a whole block
+constexpr int PLAN_THREADS = 512;
+constexpr int FENCE_MAX = 6144;      // fence entries of a heavy row (shared memory)
+constexpr int DSM_MAX = 4096;        // deletions of a heavy row cached in shared memory
 
 // ---------------------------------------------------------------------------------------
 // Staging
@@ -175,188 +181,301 @@ __global__ void k_seg_tails(const unsigned long long* __restrict__ keys, int B, 
     }
 }
 
-// Count of x in a sorted int32 span.
-__device__ __forceinline__ long long count_in(const int32_t* a, long long n, int32_t x) {
-    return upper_bound_i32(a, n, x) - lower_bound_i32(a, n, x);
-}
-
 // Deletion keys are read as neighbour ids through this view.
 struct KeySpan {
     const unsigned long long* k;
     int B;
     __device__ __forceinline__ int32_t operator[](long long i) const { return key_v(k[i], B); }
 };
-__device__ __forceinline__ long long lb_keys(KeySpan s, long long n, int32_t x) {
+template <typename S>
+__device__ __forceinline__ long long lb_span(S s, long long n, int32_t x) {
     long long lo = 0, hi = n;
     while (lo < hi) { long long mid = (lo + hi) >> 1; if (s[mid] < x) lo = mid + 1; else hi = mid; }
     return lo;
 }
-__device__ __forceinline__ long long ub_keys(KeySpan s, long long n, int32_t x) {
+template <typename S>
+__device__ __forceinline__ long long ub_span(S s, long long n, int32_t x) {
     long long lo = 0, hi = n;
     while (lo < hi) { long long mid = (lo + hi) >> 1; if (s[mid] <= x) lo = mid + 1; else hi = mid; }
     return lo;
 }
 
-// Per affected row (one warp). Multiset rule: the r-th copy of d in the deletion list cancels
-// the r-th copy of d in the old row (DeltaOverlay::removeEdge forgets one added copy or
-// tombstones the base edge, FlashGraph.h:236-243). The warp finds the old entry every
-// deletion cancels, the final position of every insertion (j + #old <= y - #cancelled <= y),
-// the new length, and only then tombstones the cancelled entries (-1) in the old row, so the
-// merge kernels stream the old row without searching it. pos is aligned with the keys.
-__global__ void k_row_plan(DGraph g, int32_t* __restrict__ pool_rw, const unsigned long long* __restrict__ keys, int B,
-                           DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
-                           const int64_t* __restrict__ seg, int64_t* __restrict__ new_len,
-                           long long* __restrict__ mdp, long long* __restrict__ pos,
-                           int32_t* __restrict__ small_list, int32_t* __restrict__ large_list) {
+// Per affected row: its descriptor before the batch, the space of its new row (old length +
+// insertions: slots of matched deletions stay unused until the next compaction), its planner
+// (warp for light rows, block for rows with many edits) and its merge slices.
+__global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
+                            const int64_t* __restrict__ seg, Row* __restrict__ old_row, int64_t* __restrict__ alloc,
+                            int32_t* __restrict__ light, int32_t* __restrict__ heavy, int64_t* __restrict__ slices,
+                            int64_t slice_cap) {
     const int A = ctr->n_aff;
-    for (int a = gwarp_id(); a < A; a += gwarp_count()) {
-        int32_t u = aff[a];
-        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
-        Row r = g.row[u];
-        const int32_t* O = g.pool + r.start;
-        KeySpan I{keys + b0, B};
-        KeySpan D{keys + sp, B};
-        long long q = e0 - sp, p = sp - b0;
+    const int T = gridDim.x * blockDim.x;
+    for (int b = (int)(blockIdx.x * blockDim.x + threadIdx.x) - (int)lane_id(); b < A; b += T) {
+        const int a = b + (int)lane_id();
+        const bool ok = a < A;
+        int ns = 0;
+        bool hv = false;
+        if (ok) {
+            long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+            Row r = row[aff[a]];
+            old_row[a] = r;
+            alloc[a] = (long long)r.len + (sp - b0);
+            hv = e0 - b0 > HEAVY_EDITS;
+            ns = r.len > 0 ? (r.len + SLICE - 1) / SLICE : 1;
+        }
+        int at_h = warp_append(ok && hv, &ctr->n_large);
+        int at_l = warp_append(ok && !hv, &ctr->n_small);
+        if (ok && hv) heavy[at_h] = a;
+        if (ok && !hv) light[at_l] = a;
+        int inc = warp_incl_scan_i(ns);
+        int base = 0;
+        if (lane_id() == WARP - 1) base = atomicAdd(&ctr->n_slices, inc);
+        base = __shfl_sync(0xffffffffu, base, WARP - 1);
+        long long s0 = (long long)base + inc - ns;
+        if (s0 + ns > slice_cap) { if (ns) atomicExch(&ctr->overflow, 1); continue; }
+        for (int s = 0; s < ns; s++) slices[s0 + s] = ((long long)a << 32) | s;
+    }
+}
+
+// Lower / upper bound in a long sorted row through a shared-memory fence of every fs-th entry:
+// the fence narrows the search to one window of fs entries.
+__device__ __forceinline__ long long fence_window(const int32_t* fence, int nf, int fs, long long len, int32_t x,
+                                                  bool upper, long long* hi_out) {
+    int lo = 0, hi = nf;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        bool go = upper ? fence[mid] <= x : fence[mid] < x;
+        if (go) lo = mid + 1; else hi = mid;
+    }
+    *hi_out = lo < nf ? (long long)lo * fs : len;
+    return lo > 0 ? (long long)(lo - 1) * fs + 1 : 0;
+}
+__device__ __forceinline__ long long lb_fence(const int32_t* O, long long len, const int32_t* fence, int nf, int fs, int32_t x) {
+    long long b, a = fence_window(fence, nf, fs, len, x, false, &b);
+    return a + lower_bound_i32(O + a, b - a, x);
+}
+__device__ __forceinline__ long long ub_fence(const int32_t* O, long long len, const int32_t* fence, int nf, int fs, int32_t x) {
+    long long b, a = fence_window(fence, nf, fs, len, x, true, &b);
+    return a + upper_bound_i32(O + a, b - a, x);
+}
+
+// Row plan. Multiset rule: the r-th copy of d in the deletion list cancels the r-th copy of d
+// in the old row (DeltaOverlay::removeEdge forgets one added copy or tombstones the base
+// edge, FlashGraph.h:236-243). For every deletion the planner records dpos = (at << 1) |
+// matched, where at is the cancelled entry, or the end of d's copies when none is left, so
+// dpos is non-decreasing along the sorted deletions, and mdp = the running count of matched
+// deletions. Every insertion y lands at j + #old <= y - #cancelled <= y of the new row and is
+// written there directly; the cancelled entries are tombstoned (-1) in the old row last, after
+// every search of the row is done. Light rows: one warp; heavy rows: one block with a fence.
+struct PlanArgs {
+    int32_t* pool;
+    Row* row;
+    const Row* old_row;
+    const unsigned long long* keys;
+    int B;
+    DevCounters* ctr;
+    const int32_t* aff;
+    const int64_t* seg;
+    const int64_t* off;
+    long long tail;
+    long long* mdp;
+    long long* dpos;
+    const int32_t* list;
+};
+
+__global__ void k_row_plan_warp(PlanArgs P) {
+    const int cnt = P.ctr->n_small;
+    long long nnz_delta = 0, bytes = 0;
+    for (int k = gwarp_id(); k < cnt; k += gwarp_count()) {
+        const int a = P.list[k];
+        const long long b0 = P.seg[3 * (int64_t)a], sp = P.seg[3 * (int64_t)a + 1], e0 = P.seg[3 * (int64_t)a + 2];
+        const Row r = P.old_row[a];
+        int32_t* O = P.pool + r.start;
+        const long long len = r.len, p = sp - b0, q = e0 - sp;
+        KeySpan I{P.keys + b0, P.B}, D{P.keys + sp, P.B};
         long long run = 0;
         for (long long base = 0; base < q; base += WARP) {
-            long long k = base + lane_id();
+            const long long k2 = base + lane_id();
             int matched = 0;
-            long long at = -1;
-            if (k < q) {
-                int32_t d = D[k];
-                long long rank = k - lb_keys(D, q, d);
-                long long lo = lower_bound_i32(O, r.len, d);
-                long long cnt = upper_bound_i32(O + lo, r.len - lo, d);
-                if (rank < cnt) { matched = 1; at = lo + rank; }
+            long long val = 0;
+            if (k2 < q) {
+                const int32_t d = D[k2];
+                const long long rank = (k2 == 0 || D[k2 - 1] != d) ? 0 : k2 - lb_span(D, q, d);
+                const long long lo = lower_bound_i32(O, len, d);
+                matched = lo + rank < len && O[lo + rank] == d;
+                const long long at = matched ? lo + rank : lo + upper_bound_i32(O + lo, len - lo, d);
+                val = (at << 1) | matched;
             }
-            int inc = warp_incl_scan_i(matched);
-            if (k < q) { mdp[sp + k] = run + inc; pos[sp + k] = at; }
+            const int inc = warp_incl_scan_i(matched);
+            if (k2 < q) { P.mdp[sp + k2] = run + inc; P.dpos[sp + k2] = val; }
             run += __shfl_sync(0xffffffffu, inc, WARP - 1);
         }
         __syncwarp();
+        int32_t* out = P.pool + P.tail + P.off[a];
         for (long long j = lane_id(); j < p; j += WARP) {
-            int32_t y = I[j];
-            long long ubo = upper_bound_i32(O, r.len, y);
-            long long ubd = ub_keys(D, q, y);
-            long long del = ubd > 0 ? mdp[sp + ubd - 1] : 0;
-            pos[b0 + j] = j + ubo - del;
+            const int32_t y = I[j];
+            const long long ubo = upper_bound_i32(O, len, y);
+            const long long ubd = ub_span(D, q, y);
+            const long long del = ubd > 0 ? P.mdp[sp + ubd - 1] : 0;
+            out[j + ubo - del] = y;
         }
         __syncwarp();
-        for (long long k = lane_id(); k < q; k += WARP) {
-            long long at = pos[sp + k];
-            if (at >= 0) pool_rw[r.start + at] = -1;
+        for (long long k2 = lane_id(); k2 < q; k2 += WARP) {
+            const long long v = P.dpos[sp + k2];
+            if (v & 1) O[v >> 1] = -1;
         }
+        const long long nl = len + p - run;
         if (lane_id() == 0) {
-            long long nl = (long long)r.len + p - run;
-            new_len[a] = nl;
-            long long work = (long long)r.len + p;
-            if (work <= SMALL_ROW_LIMIT) small_list[atomicAdd(&ctr->n_small, 1)] = a;
-            else large_list[atomicAdd(&ctr->n_large, 1)] = a;
-            atomicAdd((unsigned long long*)&ctr->nnz_delta, (unsigned long long)(nl - r.len));
-            atomicAdd((unsigned long long*)&ctr->update_bytes,
-                      (unsigned long long)(4 * (r.len + nl) + 8 * (p + q) + 16));
+            P.row[P.aff[a]] = Row{P.tail + P.off[a], (int)nl, (int)(len + p)};
+            nnz_delta += nl - len;
+            bytes += 4 * (len + nl) + 8 * (p + q) + 16;
         }
+    }
+    if (lane_id() == 0 && (nnz_delta || bytes)) {
+        atomicAdd((unsigned long long*)&P.ctr->nnz_delta, (unsigned long long)nnz_delta);
+        atomicAdd((unsigned long long*)&P.ctr->update_bytes, (unsigned long long)bytes);
     }
 }
 
-// Streams a tombstoned old row into its new place: survivor i lands at (#survivors before i)
-// + (#insertions < x); the insertion count is searched only inside the range spanned by the
-// warp's current values, which is almost always empty.
-template <int GROUP>
-__device__ __forceinline__ void merge_stream(int tid, const int32_t* __restrict__ O, long long len,
-                                             int32_t* __restrict__ out, KeySpan I, long long p,
-                                             long long* s_run, unsigned* s_cnt) {
-    long long run = 0;
-    for (long long base = 0; base < len; base += GROUP) {
-        long long i = base + tid;
-        int32_t x = i < len ? O[i] : -1;
-        bool surv = x >= 0;
-        long long lbI = 0;
-        if (p > 0) {
-            int xmin = __reduce_min_sync(0xffffffffu, surv ? x : INT32_MAX);
-            int xmax = __reduce_max_sync(0xffffffffu, surv ? x : -1);
-            long long cl = 0, ch = 0;
-            if (xmax >= 0 && lane_id() == 0) {
-                cl = lb_keys(I, p, xmin);
-                ch = lb_keys(I, p, xmax);
-            }
-            cl = __shfl_sync(0xffffffffu, cl, 0);
-            ch = __shfl_sync(0xffffffffu, ch, 0);
-            if (surv) {
-                long long lo = cl, hi = ch;
-                while (lo < hi) {
-                    long long mid = (lo + hi) >> 1;
-                    if (I[mid] < x) lo = mid + 1; else hi = mid;
-                }
-                lbI = lo;
-            }
-        }
-        unsigned m = __ballot_sync(0xffffffffu, surv);
-        long long before, chunk_total;
-        if (GROUP == WARP) {
-            before = __popc(m & ((1u << lane_id()) - 1));
-            chunk_total = __popc(m);
-        } else {
-            int w = tid / WARP;
-            if (lane_id() == 0) s_cnt[w] = __popc(m);
-            __syncthreads();
-            if (tid == 0) {
-                unsigned acc = 0;
-                for (int k = 0; k < GROUP / WARP; k++) { unsigned c = s_cnt[k]; s_cnt[k] = acc; acc += c; }
-                *s_run = acc;
-            }
-            __syncthreads();
-            before = s_cnt[w] + __popc(m & ((1u << lane_id()) - 1));
-            chunk_total = *s_run;
-            __syncthreads();
-        }
-        if (surv) out[run + before + lbI] = x;
-        run += chunk_total;
-    }
-}
-
-__global__ void k_merge_small(Row* __restrict__ row, const int32_t* __restrict__ pool_in, int32_t* __restrict__ pool_out,
-                              const unsigned long long* __restrict__ keys, int B, const DevCounters* __restrict__ ctr,
-                              const int32_t* __restrict__ aff, const int64_t* __restrict__ seg,
-                              const int64_t* __restrict__ off, const long long* __restrict__ pos,
-                              const int32_t* __restrict__ list, long long tail) {
-    const int cnt = ctr->n_small;
-    for (int k = gwarp_id(); k < cnt; k += gwarp_count()) {
-        int a = list[k];
-        int32_t u = aff[a];
-        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
-        Row r = row[u];
-        long long start = tail + off[a];
-        KeySpan I{keys + b0, B};
-        for (long long j = lane_id(); j < sp - b0; j += WARP) pool_out[start + pos[b0 + j]] = I[j];
-        merge_stream<WARP>(lane_id(), pool_in + r.start, r.len, pool_out + start, I, sp - b0, nullptr, nullptr);
-        __syncwarp();
-        int nl = (int)(off[a + 1] - off[a]);
-        if (lane_id() == 0) row[u] = Row{start, nl, nl};
-    }
-}
-
-__global__ void k_merge_large(Row* __restrict__ row, const int32_t* __restrict__ pool_in, int32_t* __restrict__ pool_out,
-                              const unsigned long long* __restrict__ keys, int B, const DevCounters* __restrict__ ctr,
-                              const int32_t* __restrict__ aff, const int64_t* __restrict__ seg,
-                              const int64_t* __restrict__ off, const long long* __restrict__ pos,
-                              const int32_t* __restrict__ list, long long tail) {
-    __shared__ long long s_run;
-    __shared__ unsigned s_cnt[LARGE_THREADS / WARP];
-    const int cnt = ctr->n_large;
+__global__ void __launch_bounds__(PLAN_THREADS) k_row_plan_block(PlanArgs P) {
+    __shared__ int32_t fence[FENCE_MAX];
+    __shared__ int32_t dval[DSM_MAX];
+    __shared__ int s_warp[PLAN_THREADS / WARP];
+    const int t = threadIdx.x, w = t / WARP;
+    const int cnt = P.ctr->n_large;
+    long long nnz_delta = 0, bytes = 0;
     for (int k = blockIdx.x; k < cnt; k += gridDim.x) {
-        int a = list[k];
-        int32_t u = aff[a];
-        long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
-        Row r = row[u];
-        long long start = tail + off[a];
+        const int a = P.list[k];
+        const long long b0 = P.seg[3 * (int64_t)a], sp = P.seg[3 * (int64_t)a + 1], e0 = P.seg[3 * (int64_t)a + 2];
+        const Row r = P.old_row[a];
+        int32_t* O = P.pool + r.start;
+        const long long len = r.len, p = sp - b0, q = e0 - sp;
+        KeySpan I{P.keys + b0, P.B}, Dg{P.keys + sp, P.B};
+        const int fs = (int)max(32LL, (len + FENCE_MAX - 1) / FENCE_MAX);
+        const int nf = (int)((len + fs - 1) / fs);
+        for (int i = t; i < nf; i += PLAN_THREADS) fence[i] = O[(long long)i * fs];
+        const bool dsm = q <= DSM_MAX;
+        if (dsm)
+            for (int i = t; i < q; i += PLAN_THREADS) dval[i] = Dg[i];
+        __syncthreads();
+        long long run = 0;
+        for (long long base = 0; base < q; base += PLAN_THREADS) {
+            const long long k2 = base + t;
+            int matched = 0;
+            long long val = 0;
+            if (k2 < q) {
+                const int32_t d = dsm ? dval[k2] : Dg[k2];
+                const int32_t dprev = k2 == 0 ? -1 : (dsm ? dval[k2 - 1] : Dg[k2 - 1]);
+                const long long rank = dprev != d ? 0 : k2 - (dsm ? lb_span(dval, q, d) : lb_span(Dg, q, d));
+                const long long lo = lb_fence(O, len, fence, nf, fs, d);
+                matched = lo + rank < len && O[lo + rank] == d;
+                const long long at = matched ? lo + rank : ub_fence(O, len, fence, nf, fs, d);
+                val = (at << 1) | matched;
+            }
+            const int inc = warp_incl_scan_i(matched);
+            if (lane_id() == WARP - 1) s_warp[w] = inc;
+            __syncthreads();
+            int before = 0, total = 0;
+            for (int i = 0; i < PLAN_THREADS / WARP; i++) {
+                const int c = s_warp[i];
+                before += i < w ? c : 0;
+                total += c;
+            }
+            if (k2 < q) { P.mdp[sp + k2] = run + before + inc; P.dpos[sp + k2] = val; }
+            run += total;
+            __syncthreads();
+        }
+        int32_t* out = P.pool + P.tail + P.off[a];
+        for (long long j = t; j < p; j += PLAN_THREADS) {
+            const int32_t y = I[j];
+            const long long ubo = ub_fence(O, len, fence, nf, fs, y);
+            const long long ubd = dsm ? ub_span(dval, q, y) : ub_span(Dg, q, y);
+            const long long del = ubd > 0 ? P.mdp[sp + ubd - 1] : 0;
+            out[j + ubo - del] = y;
+        }
+        __syncthreads();
+        for (long long k2 = t; k2 < q; k2 += PLAN_THREADS) {
+            const long long v = P.dpos[sp + k2];
+            if (v & 1) O[v >> 1] = -1;
+        }
+        const long long nl = len + p - run;
+        if (t == 0) {
+            P.row[P.aff[a]] = Row{P.tail + P.off[a], (int)nl, (int)(len + p)};
+            nnz_delta += nl - len;
+            bytes += 4 * (len + nl) + 8 * (p + q) + 16;
+        }
+        __syncthreads();
+    }
+    if (t == 0 && (nnz_delta || bytes)) {
+        atomicAdd((unsigned long long*)&P.ctr->nnz_delta, (unsigned long long)nnz_delta);
+        atomicAdd((unsigned long long*)&P.ctr->update_bytes, (unsigned long long)bytes);
+    }
+}
+
+// One warp per slice of SLICE old-row entries: streams the tombstoned entries into the new
+// row. The survivors before the slice are its start minus the matched deletions before it
+// (one search in the non-decreasing dpos); survivor x lands at (#survivors before it) +
+// (#insertions < x), the insertion count searched only inside the range spanned by the
+// chunk's values, which is almost always empty. Four coalesced loads per lane per chunk.
+__global__ void k_merge_slices(int32_t* __restrict__ pool, const unsigned long long* __restrict__ keys, int B,
+                               const DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg,
+                               const Row* __restrict__ old_row, const int64_t* __restrict__ off, long long tail,
+                               const long long* __restrict__ mdp, const long long* __restrict__ dpos,
+                               const int64_t* __restrict__ slices, int64_t slice_cap) {
+    constexpr int U = 4;
+    const long long nsl = min((long long)ctr->n_slices, (long long)slice_cap);
+    const unsigned lt = (1u << lane_id()) - 1;
+    for (long long it = gwarp_id(); it < nsl; it += gwarp_count()) {
+        const long long item = slices[it];
+        const int a = (int)(item >> 32), s = (int)(item & 0xffffffffLL);
+        const Row r = old_row[a];
+        const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+        const long long p = sp - b0, q = e0 - sp;
+        const long long s0 = (long long)s * SLICE, s1 = min((long long)r.len, s0 + SLICE);
+        if (s0 >= s1) continue;
+        long long md = 0;
+        if (q > 0 && s0 > 0 && lane_id() == 0) {
+            long long lo = 0, hi = q;
+            while (lo < hi) { long long mid = (lo + hi) >> 1; if ((dpos[sp + mid] >> 1) < s0) lo = mid + 1; else hi = mid; }
+            md = lo > 0 ? mdp[sp + lo - 1] : 0;
+        }
+        long long run = s0 - __shfl_sync(0xffffffffu, md, 0);
+        const int32_t* O = pool + r.start;
+        int32_t* out = pool + tail + off[a];
         KeySpan I{keys + b0, B};
-        for (long long j = threadIdx.x; j < sp - b0; j += LARGE_THREADS) pool_out[start + pos[b0 + j]] = I[j];
-        merge_stream<LARGE_THREADS>(threadIdx.x, pool_in + r.start, r.len, pool_out + start, I, sp - b0, &s_run, s_cnt);
-        __syncthreads();
-        int nl = (int)(off[a + 1] - off[a]);
-        if (threadIdx.x == 0) row[u] = Row{start, nl, nl};
-        __syncthreads();
+        for (long long base = s0; base < s1; base += U * WARP) {
+            int32_t x[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const long long i = base + u * WARP + lane_id();
+                x[u] = i < s1 ? O[i] : -1;
+            }
+            long long cl = 0, ch = 0;
+            if (p > 0) {
+                int xmin = INT32_MAX, xmax = -1;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (x[u] >= 0) { xmin = min(xmin, x[u]); xmax = max(xmax, x[u]); }
+                xmin = __reduce_min_sync(0xffffffffu, xmin);
+                xmax = __reduce_max_sync(0xffffffffu, xmax);
+                if (xmax >= 0 && lane_id() == 0) {
+                    cl = lb_span(I, p, xmin);
+                    ch = cl + lb_span(KeySpan{I.k + cl, B}, p - cl, xmax);
+                }
+                cl = __shfl_sync(0xffffffffu, cl, 0);
+                ch = __shfl_sync(0xffffffffu, ch, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool surv = x[u] >= 0;
+                const unsigned m = __ballot_sync(0xffffffffu, surv);
+                if (surv) {
+                    long long lbI = cl;
+                    if (ch > cl) lbI = cl + lb_span(KeySpan{I.k + cl, B}, ch - cl, x[u]);
+                    out[run + __popc(m & lt) + lbI] = x[u];
+                }
+                run += __popc(m);
+            }
+        }
     }
 }
 
@@ -368,14 +487,34 @@ __global__ void k_row_lens(const Row* __restrict__ row, int64_t n, int64_t* __re
         out[v] = row[v].len;
 }
 
-// One warp per row: copies the row to its compacted position (16-byte vector body).
+// One block per COPY_TILE entries of the compacted pool: the rows overlapping the block's
+// output range are found with one search of the new offsets, and each warp copies the
+// overlap of one row at a time, so a hub row is spread over many blocks.
+constexpr int COPY_TILE = 16384;
 __global__ void k_copy_rows(const Row* __restrict__ row, const int32_t* __restrict__ src, int32_t* __restrict__ dst,
-                            const int64_t* __restrict__ off, int32_t n) {
-    for (int v = gwarp_id(); v < n; v += gwarp_count()) {
-        Row r = row[v];
-        const int32_t* s = src + r.start;
-        int32_t* d = dst + off[v];
-        for (long long i = lane_id(); i < r.len; i += WARP) d[i] = s[i];
+                            const int64_t* __restrict__ off, int32_t n, long long live) {
+    __shared__ int s_r0, s_r1;
+    const int nw = blockDim.x / WARP, w = threadIdx.x / WARP;
+    for (long long o0 = (long long)blockIdx.x * COPY_TILE; o0 < live; o0 += (long long)gridDim.x * COPY_TILE) {
+        const long long o1 = min(live, o0 + COPY_TILE);
+        if (threadIdx.x == 0) {
+            // first row with off[r + 1] > o0, last row with off[r] < o1
+            long long lo = 0, hi = n;
+            while (lo < hi) { long long mid = (lo + hi) >> 1; if (off[mid + 1] <= o0) lo = mid + 1; else hi = mid; }
+            s_r0 = (int)lo;
+            lo = 0; hi = n;
+            while (lo < hi) { long long mid = (lo + hi) >> 1; if (off[mid] < o1) lo = mid + 1; else hi = mid; }
+            s_r1 = (int)lo;   // one past the last overlapping row
+        }
+        __syncthreads();
+        const int r0 = s_r0, r1 = s_r1;
+        for (int r = r0 + w; r < r1; r += nw) {
+            const long long b = off[r];
+            const long long a0 = max(b, o0), a1 = min((long long)off[r + 1], o1);
+            const int32_t* sr = src + row[r].start - b;
+            for (long long i = a0 + lane_id(); i < a1; i += WARP) dst[i] = sr[i];
+        }
+        __syncthreads();
     }
 }
 
@@ -406,7 +545,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     size_t sz[] = {
         (size_t)M * sizeof(scout_edge), (size_t)M, (size_t)M,
         (size_t)H * 8, (size_t)H * 8, (size_t)H * 8,
-        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)H * 4};
+        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)H * 4, (size_t)H * sizeof(Row)};
     size_t total = 0;
     for (size_t s : sz) total += align256(s);
     if (c->ws) dev_free(c, c->ws, (size_t)c->ws_bytes);
@@ -428,6 +567,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     c->d_aff_len = (int64_t*)take(sz[8]);
     c->d_aff_small = (int32_t*)take(sz[9]);
     c->d_aff_large = (int32_t*)take(sz[10]);
+    c->d_old_row = (Row*)take(sz[11]);
     c->d_hkeys = c->d_keys;
     return SCOUT_OK;
 }
@@ -467,7 +607,7 @@ int counters_fetch(scout_ctx* c) {
 int graph_ensure_scratch(scout_ctx* c) {
     if (c->stamp_a) return SCOUT_OK;
     size_t bytes = (size_t)c->n * sizeof(int32_t);
-    int32_t** arrs[] = {&c->stamp_a, &c->stamp_b, &c->stamp_c, &c->aux_v, &c->aux_w};
+    int32_t** arrs[] = {&c->stamp_a, &c->stamp_b, &c->stamp_c, &c->stamp_d, &c->aux_v, &c->aux_w};
     for (auto a : arrs) {
         SCOUT_RC(dev_alloc(c, (void**)a, bytes, "per-vertex scratch"));
         SCOUT_CU(c, cudaMemsetAsync(*a, 0, bytes, c->s_main));
@@ -476,42 +616,40 @@ int graph_ensure_scratch(scout_ctx* c) {
 }
 
 // Rewrites the pool so rows are contiguous and leaves at least min_free free elements
-// (the on-device half of compact_flash_graph).
-int graph_compact(scout_ctx* c, int64_t min_free) {
+// (the on-device half of compact_flash_graph). With nnz_exact the host's live count is used
+// and nothing waits for the device; otherwise (after staging) the live count is read back.
+int graph_compact(scout_ctx* c, int64_t min_free, bool nnz_exact) {
     const int64_t n = c->n;
-    int64_t* off = nullptr;
-    SCOUT_RC(dev_alloc(c, (void**)&off, (size_t)(n + 1) * sizeof(int64_t), "compaction offsets"));
+    if (!c->d_coff) SCOUT_RC(dev_alloc(c, (void**)&c->d_coff, (size_t)(n + 1) * sizeof(int64_t), "compaction offsets"));
+    int64_t* off = c->d_coff;
     int nb = blocks_for(n, 256);
     k_row_lens<<<nb, 256, 0, c->s_main>>>(c->row, n, off);
     SCOUT_LAUNCH(c, "k_row_lens");
-    int rc = scan_i64(c, off, n, off + n);
-    int64_t live = 0;
-    if (rc == SCOUT_OK) {
-        cudaMemcpyAsync(&live, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->s_main);
-        if (cudaStreamSynchronize(c->s_main) != cudaSuccess) rc = cuda_fail(c, cudaGetLastError(), "compaction");
+    SCOUT_RC(scan_i64(c, off, n, off + n));
+    int64_t live = c->nnz;
+    if (!nnz_exact) {
+        SCOUT_CU(c, cudaMemcpyAsync(&live, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
     }
     int64_t cap = std::max<int64_t>(c->pool_cap, live + min_free);
     // Ping-pong: the previous pool is kept as the next compaction's target, so steady-state
     // compactions allocate nothing. Without budget room for two pools the old one is freed.
     int32_t* np = nullptr;
-    if (rc == SCOUT_OK) {
-        if (c->spare && c->spare_cap >= cap) {
-            np = c->spare;
-            cap = c->spare_cap;
-            c->spare = nullptr;
-            c->spare_cap = 0;
-        } else {
-            if (c->spare) { dev_free(c, c->spare, (size_t)c->spare_cap * 4); c->spare = nullptr; c->spare_cap = 0; }
-            rc = dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool");
-        }
+    if (c->spare && c->spare_cap >= cap) {
+        np = c->spare;
+        cap = c->spare_cap;
+        c->spare = nullptr;
+        c->spare_cap = 0;
+    } else {
+        if (c->spare) { dev_free(c, c->spare, (size_t)c->spare_cap * 4); c->spare = nullptr; c->spare_cap = 0; }
+        SCOUT_RC(dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool"));
     }
-    if (rc != SCOUT_OK) { dev_free(c, off, (size_t)(n + 1) * 8); return rc; }
-    k_copy_rows<<<blocks_for(n * WARP, 256), 256, 0, c->s_main>>>(c->row, c->pool, np, off, (int32_t)n);
+    const int64_t tiles = (live + COPY_TILE - 1) / COPY_TILE;
+    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 16 * c->sm_count)), 256, 0, c->s_main>>>(
+        c->row, c->pool, np, off, (int32_t)n, (long long)live);
     k_rows_compacted<<<nb, 256, 0, c->s_main>>>(c->row, off, (int32_t)n);
     SCOUT_LAUNCH(c, "compaction");
-    c->nlaunch += 5;
-    SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
-    dev_free(c, off, (size_t)(n + 1) * 8);
+    c->nlaunch += 6;
     if (c->held <= c->budget / 100 * 85) {   // keep the old pool as the next target
         c->spare = c->pool;
         c->spare_cap = c->pool_cap;
@@ -526,16 +664,53 @@ int graph_compact(scout_ctx* c, int64_t min_free) {
     return SCOUT_OK;
 }
 
+static bool is_pinned(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Host memcpy into the pinned staging buffer, split over the host threads for large batches.
+static void stage_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t PART = (size_t)1 << 20;
+    if (bytes < 4 * PART) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const int64_t parts = (int64_t)((bytes + PART - 1) / PART);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < parts; i++) {
+        size_t o = (size_t)i * PART;
+        std::memcpy((char*)dst + o, (const char*)src + o, std::min(PART, bytes - o));
+    }
+}
+
+// Edits in pinned host memory are copied to the device directly; pageable ones go through the
+// context's pinned staging buffer.
 static int upload_edits(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m) {
-    int64_t bytes = m * (int64_t)sizeof(scout_edge) + (ops ? m : 0);
-    SCOUT_RC(pin_grow(c, &c->h_pin_edits, &c->cap_pin_edits, std::max<int64_t>(bytes, 1)));
-    std::memcpy(c->h_pin_edits, edits, (size_t)m * sizeof(scout_edge));
-    SCOUT_CU(c, cudaMemcpyAsync(c->d_edits, c->h_pin_edits, (size_t)m * sizeof(scout_edge), cudaMemcpyHostToDevice,
-                                c->s_main));
+    const size_t eb = (size_t)m * sizeof(scout_edge);
+    const bool pe = is_pinned(edits), po = !ops || is_pinned(ops);
+    if (!pe || !po) {
+        int64_t bytes = (int64_t)((pe ? 0 : eb) + (po ? 0 : (size_t)m));
+        SCOUT_RC(pin_grow(c, &c->h_pin_edits, &c->cap_pin_edits, std::max<int64_t>(bytes, 1)));
+    }
+    const void* se = edits;
+    if (!pe) {
+        stage_copy(c->h_pin_edits, edits, eb);
+        se = c->h_pin_edits;
+    }
+    SCOUT_CU(c, cudaMemcpyAsync(c->d_edits, se, eb, cudaMemcpyHostToDevice, c->s_main));
     if (ops) {
-        char* po = (char*)c->h_pin_edits + m * sizeof(scout_edge);
-        std::memcpy(po, ops, (size_t)m);
-        SCOUT_CU(c, cudaMemcpyAsync(c->d_ops, po, (size_t)m, cudaMemcpyHostToDevice, c->s_main));
+        const void* so = ops;
+        if (!po) {
+            char* dst = (char*)c->h_pin_edits + (pe ? 0 : eb);
+            stage_copy(dst, ops, (size_t)m);
+            so = dst;
+        }
+        SCOUT_CU(c, cudaMemcpyAsync(c->d_ops, so, (size_t)m, cudaMemcpyHostToDevice, c->s_main));
     }
     return SCOUT_OK;
 }
@@ -546,7 +721,7 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     c->key_bits = B;
     // Free space must hold a rewrite of every live entry plus two entries per edit.
     int64_t need = c->nnz + 2 * m + 1024;
-    if (c->pool_cap - c->tail < need) SCOUT_RC(graph_compact(c, need));
+    if (c->pool_cap - c->tail < need) SCOUT_RC(graph_compact(c, need, true));
     SCOUT_RC(ws_ensure(c, m));
     SCOUT_RC(graph_ensure_scratch(c));
     if (st) st->h2d_bytes += m * (int64_t)sizeof(scout_edge) + (ops ? m : 0);
@@ -573,21 +748,28 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_LAUNCH(c, "segments");
     c->nlaunch += 2;
     SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
-    long long* pos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
-    k_row_plan<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(g, c->pool, sorted, B, c->d_ctr, c->d_aff,
-                                                                     c->d_aff_seg, c->d_aff_len, c->d_mdp, pos,
-                                                                     c->d_aff_small, c->d_aff_large);
-    SCOUT_LAUNCH(c, "k_row_plan");
+    // merge slices: sum over affected rows of max(1, ceil(len / SLICE)) <= nnz / SLICE + Amax
+    SCOUT_RC(dev_grow(c, &c->d_slices, &c->cap_slices, c->nnz / SLICE + Amax + 1024, "merge slices"));
+    k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_old_row,
+                                                              c->d_aff_len, c->d_aff_small, c->d_aff_large, c->d_slices,
+                                                              c->cap_slices);
+    SCOUT_LAUNCH(c, "k_row_alloc");
     c->nlaunch += 1;
-    // Exclusive scan over Amax + 1 entries (the tail entries are zero), so the new length of
-    // affected row a is off[a + 1] - off[a] for every a.
+    // Exclusive scan over Amax + 1 entries (the tail entries are zero): the new row of affected
+    // row a starts at tail + off[a]; the total is this batch's pool growth.
     SCOUT_RC(scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems));
-    k_merge_small<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(
-        c->row, c->pool, c->pool, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len, pos,
-        c->d_aff_small, (long long)c->tail);
-    k_merge_large<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(Amax, 4 * c->sm_count)), LARGE_THREADS, 0,
-                    c->s_main>>>(c->row, c->pool, c->pool, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len,
-                                 pos, c->d_aff_large, (long long)c->tail);
+    long long* dpos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
+    PlanArgs pa{c->pool, c->row, c->d_old_row, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len,
+                (long long)c->tail, c->d_mdp, dpos, c->d_aff_small};
+    k_row_plan_warp<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(pa);
+    pa.list = c->d_aff_large;
+    k_row_plan_block<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(Amax, 2 * c->sm_count)), PLAN_THREADS, 0,
+                       c->s_main>>>(pa);
+    SCOUT_LAUNCH(c, "row plan");
+    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + Amax + 1024) * WARP, 256), 256, 0,
+                     c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len,
+                                  (long long)c->tail, c->d_mdp, dpos, c->d_slices, c->cap_slices);
+    c->nlaunch += 3;
     SCOUT_LAUNCH(c, "merge");
     c->nlaunch += 2;
     return SCOUT_OK;
@@ -803,7 +985,8 @@ int scout_graph_download(scout_ctx* c, int64_t* off, int32_t* adj, int64_t cap) 
     int32_t* tmp = nullptr;
     rc = dev_alloc(c, (void**)&tmp, (size_t)std::max<int64_t>(total, 1) * 4, "download buffer");
     if (rc != SCOUT_OK) { dev_free(c, d_off, (size_t)(n + 1) * 8); return rc; }
-    k_copy_rows<<<blocks_for(n * WARP, 256), 256, 0, c->s_main>>>(c->row, c->pool, tmp, d_off, (int32_t)n);
+    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((total + COPY_TILE - 1) / COPY_TILE, 16 * c->sm_count)),
+                  256, 0, c->s_main>>>(c->row, c->pool, tmp, d_off, (int32_t)n, (long long)total);
     cudaMemcpyAsync(adj, tmp, (size_t)total * 4, cudaMemcpyDeviceToHost, c->s_main);
     cudaError_t e = cudaStreamSynchronize(c->s_main);
     dev_free(c, tmp, (size_t)std::max<int64_t>(total, 1) * 4);
@@ -816,7 +999,7 @@ int scout_graph_compact(scout_ctx* c) {
     if (!c) return SCOUT_E_INVALID;
     if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
     cudaSetDevice(c->device);
-    return graph_compact(c, std::max<int64_t>(c->nnz, 1 << 22));
+    return graph_compact(c, std::max<int64_t>(c->nnz, 1 << 22), true);
 }
 
 int scout_classify(scout_ctx* c, const scout_edge* e, int64_t m, uint8_t* out) {

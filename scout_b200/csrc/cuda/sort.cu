@@ -1,9 +1,9 @@
 // sort.cu -- stable LSD radix sort of 64-bit keys and an exclusive int64 scan.
 //
 // The batch merge groups half-edits by (vertex, op, neighbour) with one sort. Small sorts run
-// in one CTA entirely in shared memory (one launch); larger ones take three launches per
-// 8-bit digit: tile histograms, one scan of the digit-major histogram, and a stable scatter
-// that ranks equal digits inside a warp with __match_any_sync.
+// in one CTA entirely in shared memory (one launch); larger ones take, per 8-bit digit, tile
+// histograms, a three-kernel scan of the digit-major histogram, and a stable scatter that
+// ranks equal digits inside a warp with __match_any_sync.
 #include "ctx.cuh"
 
 namespace scout {
@@ -31,29 +31,6 @@ __global__ void k_sort_hist(const unsigned long long* __restrict__ keys, int64_t
     for (int d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) hist[(int64_t)d * nblocks + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of a uint32 array with one block (used on digit-major tile histograms).
-__global__ void k_scan_u32_single(unsigned int* __restrict__ a, int64_t n) {
-    __shared__ unsigned long long part[1024];
-    int t = threadIdx.x, T = blockDim.x;
-    int64_t per = (n + T - 1) / T;
-    int64_t lo = (int64_t)t * per, hi = lo + per < n ? lo + per : n;
-    unsigned long long s = 0;
-    for (int64_t i = lo; i < hi; i++) s += a[i];
-    part[t] = s;
-    __syncthreads();
-    for (int o = 1; o < T; o <<= 1) {
-        unsigned long long y = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += y;
-        __syncthreads();
-    }
-    unsigned long long run = part[t] - s;
-    for (int64_t i = lo; i < hi; i++) {
-        unsigned int x = a[i];
-        a[i] = (unsigned int)run;
-        run += x;
-    }
-}
 
 // Stable scatter of one tile: chunks of 256 keys, warp ranks via __match_any_sync, cross-warp
 // offsets from a per-warp digit table.
@@ -149,41 +126,8 @@ __global__ void k_sort_small(unsigned long long* __restrict__ keys, int n, int b
     for (int i = t; i < n; i += blockDim.x) keys[i] = a[i];
 }
 
-int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, int64_t n, int bits,
-              unsigned long long** sorted_out) {
-    *sorted_out = keys;
-    if (n <= 1) return SCOUT_OK;
-    if (n <= SMALL_SORT_MAX) {
-        constexpr int NW = SMALL_SORT_THREADS / WARP;
-        size_t smem = 2 * (size_t)n * sizeof(unsigned long long) + (size_t)(NW + 1) * SORT_RADIX * sizeof(unsigned);
-        static bool attr_set = false;
-        if (!attr_set) {
-            SCOUT_CU(c, cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-            attr_set = true;
-        }
-        k_sort_small<<<1, SMALL_SORT_THREADS, smem, c->s_main>>>(keys, (int)n, bits);
-        SCOUT_LAUNCH(c, "k_sort_small");
-        c->nlaunch += 1;
-        return SCOUT_OK;
-    }
-    int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
-    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, (int64_t)nblocks * SORT_RADIX, "sort histogram"));
-    unsigned long long* src = keys;
-    unsigned long long* dst = alt;
-    for (int shift = 0; shift < bits; shift += 8) {
-        k_sort_hist<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, n, shift, c->d_sort_hist, nblocks);
-        k_scan_u32_single<<<1, 1024, 0, c->s_main>>>(c->d_sort_hist, (int64_t)nblocks * SORT_RADIX);
-        k_sort_scatter<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, dst, n, shift, c->d_sort_hist, nblocks);
-        SCOUT_LAUNCH(c, "radix pass");
-        c->nlaunch += 3;
-        unsigned long long* s = src; src = dst; dst = s;
-    }
-    *sorted_out = src;
-    return SCOUT_OK;
-}
-
 // ---------------------------------------------------------------------------------------
-// Exclusive int64 scan: tile sums, one-block scan of the sums, tile scans with offsets.
+// Exclusive scans: tile sums, one-block scan of the sums, tile scans with offsets.
 // ---------------------------------------------------------------------------------------
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 8;
@@ -207,11 +151,12 @@ __device__ __forceinline__ long long block_excl_scan(long long x, long long* tot
     return r;
 }
 
-__global__ void k_scan_tiles(const int64_t* __restrict__ a, int64_t n, int64_t* __restrict__ sums) {
+template <typename T>
+__global__ void k_scan_tiles(const T* __restrict__ a, int64_t n, int64_t* __restrict__ sums) {
     int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     long long s = 0;
     for (int k = 0; k < SCAN_ITEMS; k++)
-        if (base + k < n) s += a[base + k];
+        if (base + k < n) s += (long long)a[base + k];
     __shared__ long long tot;
     block_excl_scan(s, &tot);
     __syncthreads();
@@ -242,33 +187,70 @@ __global__ void k_scan_sums(int64_t* __restrict__ sums, int64_t nb, int64_t* __r
     if (t == T - 1 && d_total) *d_total = part[T - 1];
 }
 
-__global__ void k_scan_apply(int64_t* __restrict__ a, int64_t n, const int64_t* __restrict__ sums) {
+template <typename T>
+__global__ void k_scan_apply(T* __restrict__ a, int64_t n, const int64_t* __restrict__ sums) {
     int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     long long v[SCAN_ITEMS];
     long long s = 0;
     for (int k = 0; k < SCAN_ITEMS; k++) {
-        v[k] = base + k < n ? a[base + k] : 0;
+        v[k] = base + k < n ? (long long)a[base + k] : 0;
         s += v[k];
     }
     long long ex = block_excl_scan(s, nullptr) + sums[blockIdx.x];
     for (int k = 0; k < SCAN_ITEMS; k++) {
-        if (base + k < n) a[base + k] = ex;
+        if (base + k < n) a[base + k] = (T)ex;
         ex += v[k];
     }
 }
 
-int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total) {
+template <typename T>
+static int scan_any(scout_ctx* c, T* data, int64_t n, int64_t* d_total) {
     if (n <= 0) {
         if (d_total) SCOUT_CU(c, cudaMemsetAsync(d_total, 0, sizeof(int64_t), c->s_main));
         return SCOUT_OK;
     }
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, nb + 1, "scan partials"));
-    k_scan_tiles<<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
+    k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
     k_scan_sums<<<1, 1024, 0, c->s_main>>>(c->d_scan_tmp, nb, d_total);
-    k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
-    SCOUT_LAUNCH(c, "scan_i64");
+    k_scan_apply<T><<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
+    SCOUT_LAUNCH(c, "scan");
     c->nlaunch += 3;
+    return SCOUT_OK;
+}
+
+int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total) { return scan_any(c, data, n, d_total); }
+
+int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, int64_t n, int bits,
+              unsigned long long** sorted_out) {
+    *sorted_out = keys;
+    if (n <= 1) return SCOUT_OK;
+    if (n <= SMALL_SORT_MAX) {
+        constexpr int NW = SMALL_SORT_THREADS / WARP;
+        size_t smem = 2 * (size_t)n * sizeof(unsigned long long) + (size_t)(NW + 1) * SORT_RADIX * sizeof(unsigned);
+        static bool attr_set = false;
+        if (!attr_set) {
+            SCOUT_CU(c, cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+            attr_set = true;
+        }
+        k_sort_small<<<1, SMALL_SORT_THREADS, smem, c->s_main>>>(keys, (int)n, bits);
+        SCOUT_LAUNCH(c, "k_sort_small");
+        c->nlaunch += 1;
+        return SCOUT_OK;
+    }
+    int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
+    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, (int64_t)nblocks * SORT_RADIX, "sort histogram"));
+    unsigned long long* src = keys;
+    unsigned long long* dst = alt;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_sort_hist<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, n, shift, c->d_sort_hist, nblocks);
+        SCOUT_RC(scan_any(c, c->d_sort_hist, (int64_t)nblocks * SORT_RADIX, nullptr));
+        k_sort_scatter<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, dst, n, shift, c->d_sort_hist, nblocks);
+        SCOUT_LAUNCH(c, "radix pass");
+        c->nlaunch += 2;
+        unsigned long long* s = src; src = dst; dst = s;
+    }
+    *sorted_out = src;
     return SCOUT_OK;
 }
 

@@ -12,6 +12,7 @@ text-format I/O, and the storage-resident hybrid graph.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -61,6 +62,26 @@ def as_edges(e) -> np.ndarray:
     if a.ndim != 2 or a.shape[1] != 2:
         raise ValueError("edges must have shape (m, 2)")
     return a
+
+
+def pinned_empty(shape, dtype=np.int32) -> np.ndarray:
+    """An uninitialised array in page-locked host memory (scout_host_alloc): edit batches in
+    such memory are copied to the device without the staging copy."""
+    dt = np.dtype(dtype)
+    count = int(np.prod(shape)) if np.ndim(shape) else int(shape)
+    nbytes = max(count * dt.itemsize, 1)
+    ptr = C.c_void_p()
+    _check(LIB.scout_host_alloc(nbytes, C.byref(ptr)))
+    buf = (C.c_uint8 * nbytes).from_address(ptr.value)
+    weakref.finalize(buf, LIB.scout_host_free, ptr.value)
+    return np.frombuffer(buf, dtype=dt, count=count).reshape(shape)
+
+
+def pinned_copy(a) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    out = pinned_empty(a.shape, a.dtype)
+    out[...] = a
+    return out
 
 
 def device_count() -> int:
