@@ -99,8 +99,8 @@ struct scout_ctx {
     int32_t* d_aff = nullptr;       // affected vertex ids (2m)
     int64_t* d_aff_seg = nullptr;   // [3 * 2m]: segment begin, first deletion, end
     int64_t* d_aff_len = nullptr;   // new length, then exclusive offsets (2m + 1)
-    int32_t* d_aff_small = nullptr; // rows planned by a warp (2m)
-    int32_t* d_aff_large = nullptr; // rows planned by a block (2m)
+    int32_t* d_aff_small = nullptr; // affected rows merged by the short-row merge (2m)
+    int64_t* d_small_off = nullptr; // short-row lengths, then their exclusive scan (2m + 1)
     scout::Row* d_old_row = nullptr;   // descriptors of the affected rows before the batch (2m)
     int64_t* d_slices = nullptr;  int64_t cap_slices = 0;   // merge items (row << 32 | slice)
     int64_t* d_coff = nullptr;      // compaction offsets (n + 1)

@@ -15,12 +15,16 @@
 //                     keys (u, op, v) and (v, op, u) per applied edit
 //   sort_keys         groups half-edits by vertex; inserts before deletes; neighbours sorted
 //   k_seg_heads/tails affected-vertex list and its key segments
-//   k_row_alloc       old descriptor, new space (old length + insertions), planner, slices
+//   k_row_alloc       old descriptor, new space (old length + insertions), short-row list,
+//                     slices of long rows
 //   scan_i64          new rows' offsets in the pool
-//   k_row_plan_*      matched deletions (multiset cancel, tombstoned in the old row), new
-//                     length, insertions written to their final slots; warp or block per row
-//   k_merge_slices    survivors of the old row streamed into the new row, one warp per slice
-//                     of SLICE entries, so a hub row is spread over many warps
+//   k_plan_match      per deletion: the old entry it cancels (multiset rule); matched flags
+//   scan_i64          matched deletions before every half-edit
+//   k_plan_place      per insertion: its final slot in the new row; per matched deletion: the
+//                     old entry's tombstone (sign bit); per row: the new descriptor
+//   k_merge_small     survivors of short rows, balanced groups of ~UNIT entries per warp
+//   k_merge_slices    survivors of long rows, one warp per slice of SLICE entries, so a hub
+//                     row is spread over many warps
 #include "ctx.cuh"
 
 #include <algorithm>
@@ -28,11 +32,8 @@
 
 namespace scout {
 
-constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the merge
-constexpr int HEAVY_EDITS = 64;      // rows with more half-edits are planned by a whole block
-constexpr int PLAN_THREADS = 512;
-constexpr int FENCE_MAX = 6144;      // fence entries of a heavy row (shared memory)
-constexpr int DSM_MAX = 4096;        // deletions of a heavy row cached in shared memory
+constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the long-row merge
+constexpr int SMALL_LEN = 2048;      // rows up to this length go to the short-row merge
 
 // ---------------------------------------------------------------------------------------
 // Staging
@@ -200,12 +201,31 @@ __device__ __forceinline__ long long ub_span(S s, long long n, int32_t x) {
     return lo;
 }
 
-// Per affected row: its descriptor before the batch, the space of its new row (old length +
-// insertions: slots of matched deletions stay unused until the next compaction), its planner
-// (warp for light rows, block for rows with many edits) and its merge slices.
+__device__ __forceinline__ long long warp_lower_bound(const int64_t* a, long long n, long long x) {
+    // first i in [0, n) with a[i] >= x (n if none), 32 probes per step (all lanes call)
+    long long lo = 0, hi = n;
+    while (hi - lo > WARP) {
+        const long long step = (hi - lo + WARP - 1) / WARP;
+        const long long pos = lo + (long long)lane_id() * step;
+        const bool less = pos < hi && a[pos] < x;
+        const int c = __popc(__ballot_sync(0xffffffffu, less));   // probes below x form a prefix
+        const long long nlo = c == 0 ? lo : lo + (long long)(c - 1) * step + 1;
+        const long long nhi = c == 0 ? lo : min(hi, lo + (long long)c * step);
+        lo = nlo;
+        hi = max(nlo, nhi);
+        if (c == 0) break;
+    }
+    const long long pos = lo + lane_id();
+    const bool less = pos < hi && a[pos] < x;
+    return lo + __popc(__ballot_sync(0xffffffffu, less));
+}
+
+// Per affected row: its descriptor before the batch and the space of its new row (old length
+// + insertions: slots of matched deletions stay unused until the next compaction). Rows up
+// to SMALL_LEN entries go to the short-row merge, longer ones are cut into merge slices.
 __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
                             const int64_t* __restrict__ seg, Row* __restrict__ old_row, int64_t* __restrict__ alloc,
-                            int32_t* __restrict__ light, int32_t* __restrict__ heavy, int64_t* __restrict__ slices,
+                            int32_t* __restrict__ small, int64_t* __restrict__ small_len, int64_t* __restrict__ slices,
                             int64_t slice_cap) {
     const int A = ctr->n_aff;
     const int T = gridDim.x * blockDim.x;
@@ -213,213 +233,240 @@ __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict
         const int a = b + (int)lane_id();
         const bool ok = a < A;
         int ns = 0;
-        bool hv = false;
+        bool sm = false;
         if (ok) {
-            long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
-            Row r = row[aff[a]];
+            const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
+            const Row r = row[aff[a]];
             old_row[a] = r;
             alloc[a] = (long long)r.len + (sp - b0);
-            hv = e0 - b0 > HEAVY_EDITS;
-            ns = r.len > 0 ? (r.len + SLICE - 1) / SLICE : 1;
+            sm = r.len <= SMALL_LEN;
+            ns = sm ? 0 : (r.len + SLICE - 1) / SLICE;
         }
-        int at_h = warp_append(ok && hv, &ctr->n_large);
-        int at_l = warp_append(ok && !hv, &ctr->n_small);
-        if (ok && hv) heavy[at_h] = a;
-        if (ok && !hv) light[at_l] = a;
-        int inc = warp_incl_scan_i(ns);
+        const int at = warp_append(ok && sm, &ctr->n_small);
+        if (ok && sm) {
+            small[at] = a;
+            small_len[at] = alloc[a] - (seg[3 * (int64_t)a + 1] - seg[3 * (int64_t)a]);   // the old length
+        }
+        const int inc = warp_incl_scan_i(ns);
         int base = 0;
-        if (lane_id() == WARP - 1) base = atomicAdd(&ctr->n_slices, inc);
+        if (lane_id() == WARP - 1 && inc) base = atomicAdd(&ctr->n_slices, inc);
         base = __shfl_sync(0xffffffffu, base, WARP - 1);
-        long long s0 = (long long)base + inc - ns;
+        const long long s0 = (long long)base + inc - ns;
         if (s0 + ns > slice_cap) { if (ns) atomicExch(&ctr->overflow, 1); continue; }
         for (int s = 0; s < ns; s++) slices[s0 + s] = ((long long)a << 32) | s;
     }
 }
 
-// Lower / upper bound in a long sorted row through a shared-memory fence of every fs-th entry:
-// the fence narrows the search to one window of fs entries.
-__device__ __forceinline__ long long fence_window(const int32_t* fence, int nf, int fs, long long len, int32_t x,
-                                                  bool upper, long long* hi_out) {
-    int lo = 0, hi = nf;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        bool go = upper ? fence[mid] <= x : fence[mid] < x;
-        if (go) lo = mid + 1; else hi = mid;
+// Searches of an old row whose cancelled entries may already carry the tombstone bit (the
+// sign bit, so the masked values stay sorted while the row is being marked).
+__device__ __forceinline__ int32_t unmark(int32_t x) { return x & 0x7fffffff; }
+__device__ __forceinline__ long long ub_masked(const int32_t* a, long long n, int32_t x) {
+    long long lo = 0, hi = n;
+    while (lo < hi) { long long mid = (lo + hi) >> 1; if (unmark(a[mid]) <= x) lo = mid + 1; else hi = mid; }
+    return lo;
+}
+
+// Plan, step 1: one thread per half-edit. Multiset rule: the r-th copy of d among a row's
+// deletions cancels the r-th copy of d in the old row (DeltaOverlay::removeEdge forgets one
+// added copy or tombstones the base edge, FlashGraph.h:236-243). A deletion records dpos =
+// (at << 1) | matched, with at the cancelled entry, or the end of d's copies when none is
+// left, so dpos is non-decreasing along a row's sorted deletions; flag = matched (0 for
+// insertions and for the unused tail up to H) feeds one exclusive scan over all half-edits.
+__global__ void k_plan_match(const int32_t* __restrict__ pool, const unsigned long long* __restrict__ keys, int B,
+                             const DevCounters* __restrict__ ctr, const int32_t* __restrict__ slot,
+                             const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
+                             long long* __restrict__ dpos, long long* __restrict__ flag, long long H) {
+    const long long nh = ctr->n_half;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < H; k += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = k < nh ? keys[k] : 0ull;
+        long long f = 0;
+        if (k < nh && key_op(key, B) == 1) {
+            const int a = slot[key_u(key, B)];
+            const long long sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+            const int32_t d = key_v(key, B);
+            long long rank = 0;
+            if (k > sp && key_v(keys[k - 1], B) == d) rank = k - (sp + lb_span(KeySpan{keys + sp, B}, e0 - sp, d));
+            const Row r = old_row[a];
+            const int32_t* O = pool + r.start;
+            const long long lo = lower_bound_i32(O, r.len, d);
+            const bool matched = lo + rank < r.len && O[lo + rank] == d;
+            const long long at = matched ? lo + rank : lo + upper_bound_i32(O + lo, r.len - lo, d);
+            dpos[k] = (at << 1) | (matched ? 1 : 0);
+            f = matched ? 1 : 0;
+        }
+        flag[k] = f;
     }
-    *hi_out = lo < nf ? (long long)lo * fs : len;
-    return lo > 0 ? (long long)(lo - 1) * fs + 1 : 0;
-}
-__device__ __forceinline__ long long lb_fence(const int32_t* O, long long len, const int32_t* fence, int nf, int fs, int32_t x) {
-    long long b, a = fence_window(fence, nf, fs, len, x, false, &b);
-    return a + lower_bound_i32(O + a, b - a, x);
-}
-__device__ __forceinline__ long long ub_fence(const int32_t* O, long long len, const int32_t* fence, int nf, int fs, int32_t x) {
-    long long b, a = fence_window(fence, nf, fs, len, x, true, &b);
-    return a + upper_bound_i32(O + a, b - a, x);
 }
 
-// Row plan. Multiset rule: the r-th copy of d in the deletion list cancels the r-th copy of d
-// in the old row (DeltaOverlay::removeEdge forgets one added copy or tombstones the base
-// edge, FlashGraph.h:236-243). For every deletion the planner records dpos = (at << 1) |
-// matched, where at is the cancelled entry, or the end of d's copies when none is left, so
-// dpos is non-decreasing along the sorted deletions, and mdp = the running count of matched
-// deletions. Every insertion y lands at j + #old <= y - #cancelled <= y of the new row and is
-// written there directly; the cancelled entries are tombstoned (-1) in the old row last, after
-// every search of the row is done. Light rows: one warp; heavy rows: one block with a fence.
-struct PlanArgs {
-    int32_t* pool;
-    Row* row;
-    const Row* old_row;
-    const unsigned long long* keys;
-    int B;
-    DevCounters* ctr;
-    const int32_t* aff;
-    const int64_t* seg;
-    const int64_t* off;
-    long long tail;
-    long long* mdp;
-    long long* dpos;
-    const int32_t* list;
-};
-
-__global__ void k_row_plan_warp(PlanArgs P) {
-    const int cnt = P.ctr->n_small;
+// Plan, step 2 (after the scan: E[k] = matched deletions before half-edit k): one thread per
+// half-edit. An insertion y (j-th of its row) lands at j + #old <= y - #cancelled <= y of the
+// new row and is written there; a matched deletion tombstones its old entry; the first
+// half-edit of a row writes the row's new descriptor.
+__global__ void k_plan_place(int32_t* __restrict__ pool, Row* __restrict__ row, const unsigned long long* __restrict__ keys,
+                             int B, DevCounters* __restrict__ ctr, const int32_t* __restrict__ slot,
+                             const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
+                             const int64_t* __restrict__ off, long long tail, const long long* __restrict__ dpos,
+                             const long long* __restrict__ E) {
+    const long long nh = ctr->n_half;
     long long nnz_delta = 0, bytes = 0;
-    for (int k = gwarp_id(); k < cnt; k += gwarp_count()) {
-        const int a = P.list[k];
-        const long long b0 = P.seg[3 * (int64_t)a], sp = P.seg[3 * (int64_t)a + 1], e0 = P.seg[3 * (int64_t)a + 2];
-        const Row r = P.old_row[a];
-        int32_t* O = P.pool + r.start;
-        const long long len = r.len, p = sp - b0, q = e0 - sp;
-        KeySpan I{P.keys + b0, P.B}, D{P.keys + sp, P.B};
-        long long run = 0;
-        for (long long base = 0; base < q; base += WARP) {
-            const long long k2 = base + lane_id();
-            int matched = 0;
-            long long val = 0;
-            if (k2 < q) {
-                const int32_t d = D[k2];
-                const long long rank = (k2 == 0 || D[k2 - 1] != d) ? 0 : k2 - lb_span(D, q, d);
-                const long long lo = lower_bound_i32(O, len, d);
-                matched = lo + rank < len && O[lo + rank] == d;
-                const long long at = matched ? lo + rank : lo + upper_bound_i32(O + lo, len - lo, d);
-                val = (at << 1) | matched;
-            }
-            const int inc = warp_incl_scan_i(matched);
-            if (k2 < q) { P.mdp[sp + k2] = run + inc; P.dpos[sp + k2] = val; }
-            run += __shfl_sync(0xffffffffu, inc, WARP - 1);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nh; k += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[k];
+        const int32_t u = key_u(key, B);
+        const int a = slot[u];
+        const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1], e0 = seg[3 * (int64_t)a + 2];
+        const Row r = old_row[a];
+        int32_t* O = pool + r.start;
+        if (k < sp) {
+            const int32_t y = key_v(key, B);
+            const long long ubo = ub_masked(O, r.len, y);
+            const long long ubd = ub_span(KeySpan{keys + sp, B}, e0 - sp, y);
+            const long long del = E[sp + ubd] - E[sp];
+            pool[tail + off[a] + (k - b0) + ubo - del] = y;
+        } else {
+            const long long dp = dpos[k];
+            if (dp & 1) O[dp >> 1] = key_v(key, B) | (int32_t)0x80000000;
         }
-        __syncwarp();
-        int32_t* out = P.pool + P.tail + P.off[a];
-        for (long long j = lane_id(); j < p; j += WARP) {
-            const int32_t y = I[j];
-            const long long ubo = upper_bound_i32(O, len, y);
-            const long long ubd = ub_span(D, q, y);
-            const long long del = ubd > 0 ? P.mdp[sp + ubd - 1] : 0;
-            out[j + ubo - del] = y;
+        if (k == b0) {
+            const long long p = sp - b0, q = e0 - sp;
+            const long long nl = (long long)r.len + p - (E[e0] - E[sp]);
+            row[u] = Row{tail + off[a], (int)nl, (int)(r.len + p)};
+            nnz_delta += nl - r.len;
+            bytes += 4 * (r.len + nl) + 8 * (p + q) + 16;
         }
-        __syncwarp();
-        for (long long k2 = lane_id(); k2 < q; k2 += WARP) {
-            const long long v = P.dpos[sp + k2];
-            if (v & 1) O[v >> 1] = -1;
-        }
-        const long long nl = len + p - run;
-        if (lane_id() == 0) {
-            P.row[P.aff[a]] = Row{P.tail + P.off[a], (int)nl, (int)(len + p)};
-            nnz_delta += nl - len;
-            bytes += 4 * (len + nl) + 8 * (p + q) + 16;
-        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nnz_delta += __shfl_xor_sync(__activemask(), nnz_delta, o);
+        bytes += __shfl_xor_sync(__activemask(), bytes, o);
     }
     if (lane_id() == 0 && (nnz_delta || bytes)) {
-        atomicAdd((unsigned long long*)&P.ctr->nnz_delta, (unsigned long long)nnz_delta);
-        atomicAdd((unsigned long long*)&P.ctr->update_bytes, (unsigned long long)bytes);
+        atomicAdd((unsigned long long*)&ctr->nnz_delta, (unsigned long long)nnz_delta);
+        atomicAdd((unsigned long long*)&ctr->update_bytes, (unsigned long long)bytes);
     }
 }
 
-__global__ void __launch_bounds__(PLAN_THREADS) k_row_plan_block(PlanArgs P) {
-    __shared__ int32_t fence[FENCE_MAX];
-    __shared__ int32_t dval[DSM_MAX];
-    __shared__ int s_warp[PLAN_THREADS / WARP];
-    const int t = threadIdx.x, w = t / WARP;
-    const int cnt = P.ctr->n_large;
-    long long nnz_delta = 0, bytes = 0;
-    for (int k = blockIdx.x; k < cnt; k += gridDim.x) {
-        const int a = P.list[k];
-        const long long b0 = P.seg[3 * (int64_t)a], sp = P.seg[3 * (int64_t)a + 1], e0 = P.seg[3 * (int64_t)a + 2];
-        const Row r = P.old_row[a];
-        int32_t* O = P.pool + r.start;
-        const long long len = r.len, p = sp - b0, q = e0 - sp;
-        KeySpan I{P.keys + b0, P.B}, Dg{P.keys + sp, P.B};
-        const int fs = (int)max(32LL, (len + FENCE_MAX - 1) / FENCE_MAX);
-        const int nf = (int)((len + fs - 1) / fs);
-        for (int i = t; i < nf; i += PLAN_THREADS) fence[i] = O[(long long)i * fs];
-        const bool dsm = q <= DSM_MAX;
-        if (dsm)
-            for (int i = t; i < q; i += PLAN_THREADS) dval[i] = Dg[i];
-        __syncthreads();
-        long long run = 0;
-        for (long long base = 0; base < q; base += PLAN_THREADS) {
-            const long long k2 = base + t;
-            int matched = 0;
-            long long val = 0;
-            if (k2 < q) {
-                const int32_t d = dsm ? dval[k2] : Dg[k2];
-                const int32_t dprev = k2 == 0 ? -1 : (dsm ? dval[k2 - 1] : Dg[k2 - 1]);
-                const long long rank = dprev != d ? 0 : k2 - (dsm ? lb_span(dval, q, d) : lb_span(Dg, q, d));
-                const long long lo = lb_fence(O, len, fence, nf, fs, d);
-                matched = lo + rank < len && O[lo + rank] == d;
-                const long long at = matched ? lo + rank : ub_fence(O, len, fence, nf, fs, d);
-                val = (at << 1) | matched;
+// Short rows, balanced: the short rows' old lengths are scanned (soff) and cut into groups of
+// about UNIT entries (a row belongs to the group its first entry falls in), one warp per
+// group. The warp takes the group's rows 32 at a time, one row per lane, and streams their
+// entries 32 at a time, every lane finding its row by a search over the lanes' prefix sums.
+// A surviving entry x lands at (survivors of its row before it) + (#insertions of its row
+// < x); the insertion values of the 32 rows are staged in shared memory when they fit, and
+// per-row survivor counts carry across chunks in shared memory.
+constexpr int MERGE_THREADS = 256;
+constexpr int UNIT = 1024;
+constexpr int ICAP = 512;
+
+__global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
+        int32_t* __restrict__ pool, const unsigned long long* __restrict__ keys, int B,
+        const DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
+        const int64_t* __restrict__ off, long long tail, const int32_t* __restrict__ small,
+        const int64_t* __restrict__ soff) {
+    __shared__ int s_cnt[MERGE_THREADS / WARP][WARP];
+    __shared__ int32_t s_ins[MERGE_THREADS / WARP][ICAP];
+    const int w = threadIdx.x / WARP;
+    const unsigned lane = lane_id();
+    const int ns = ctr->n_small;
+    const long long total = soff[ns];
+    const long long G = (total + UNIT - 1) / UNIT;
+    for (long long g = gwarp_id(); g < G; g += gwarp_count()) {
+        const long long i0 = warp_lower_bound(soff, ns, g * UNIT);
+        const long long i1 = warp_lower_bound(soff, ns, (g + 1) * UNIT);
+        for (long long rb = i0; rb < i1; rb += WARP) {
+            const long long i = rb + lane;
+            long long st = 0, ob = 0, ib = 0;
+            int len = 0, p = 0;
+            if (i < i1) {
+                const int a = small[i];
+                const Row r = old_row[a];
+                st = r.start;
+                len = r.len;
+                ib = seg[3 * (int64_t)a];
+                p = (int)(seg[3 * (int64_t)a + 1] - ib);
+                ob = tail + off[a];
             }
-            const int inc = warp_incl_scan_i(matched);
-            if (lane_id() == WARP - 1) s_warp[w] = inc;
-            __syncthreads();
-            int before = 0, total = 0;
-            for (int i = 0; i < PLAN_THREADS / WARP; i++) {
-                const int c = s_warp[i];
-                before += i < w ? c : 0;
-                total += c;
+            s_cnt[w][lane] = 0;
+            const int pin = warp_incl_scan_i(p);
+            const int ptot = __shfl_sync(0xffffffffu, pin, WARP - 1);
+            const int pex = pin - p;
+            const bool staged = ptot <= ICAP;
+            if (staged)
+                for (int t = 0; t < p; t++) s_ins[w][pex + t] = key_v(keys[ib + t], B);
+            __syncwarp();
+            const int incl = warp_incl_scan_i(len);
+            const int tot = __shfl_sync(0xffffffffu, incl, WARP - 1);
+            const int excl = incl - len;
+            constexpr int U = 4;   // chunks per step: their loads are issued before any store
+            for (int e00 = 0; e00 < tot; e00 += U * WARP) {
+                int jj[U];
+                int32_t xx[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int e = e00 + u * WARP + (int)lane;
+                    int lo = 0, hi = WARP - 1;
+#pragma unroll
+                    for (int it = 0; it < 5; it++) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (__shfl_sync(0xffffffffu, excl, mid) <= e) lo = mid; else hi = mid - 1;
+                    }
+                    jj[u] = lo;
+                    const int ej = __shfl_sync(0xffffffffu, excl, lo);
+                    const long long sj = __shfl_sync(0xffffffffu, st, lo);
+                    xx[u] = e < tot ? pool[sj + (e - ej)] : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int e0 = e00 + u * WARP;
+                    if (e0 >= tot) break;   // uniform
+                    const int j = jj[u];
+                    const int32_t x = xx[u];
+                    const int e = e0 + (int)lane;
+                    const int ej = __shfl_sync(0xffffffffu, excl, j);
+                    const int lj = __shfl_sync(0xffffffffu, len, j);
+                    const long long oj = __shfl_sync(0xffffffffu, ob, j);
+                    const long long ij = __shfl_sync(0xffffffffu, ib, j);
+                    const int pj = __shfl_sync(0xffffffffu, p, j);
+                    const int xj = __shfl_sync(0xffffffffu, pex, j);
+                    const bool in = e < tot;
+                    const bool surv = x >= 0;
+                    const unsigned m = __ballot_sync(0xffffffffu, surv);
+                    const int fl = max(ej - e0, 0);                    // first lane of row j in this chunk
+                    const int ll = min(ej + lj - e0, WARP) - 1;        // last lane of row j in this chunk
+                    const unsigned below = (1u << lane) - 1;
+                    const unsigned from_fl = ~((1u << fl) - 1);
+                    if (surv) {
+                        int lbI = 0;
+                        if (pj > 0) {
+                            if (staged) {
+                                int a = 0, b = pj;
+                                while (a < b) { int mid = (a + b) >> 1; if (s_ins[w][xj + mid] < x) a = mid + 1; else b = mid; }
+                                lbI = a;
+                            } else {
+                                lbI = (int)lb_span(KeySpan{keys + ij, B}, pj, x);
+                            }
+                        }
+                        pool[oj + s_cnt[w][j] + __popc(m & below & from_fl) + lbI] = x;
+                    }
+                    __syncwarp();
+                    if (in && (int)lane == ll) {
+                        const unsigned upto = ll >= WARP - 1 ? 0xffffffffu : ((1u << (ll + 1)) - 1);
+                        s_cnt[w][j] += __popc(m & upto & from_fl);
+                    }
+                    __syncwarp();
+                }
             }
-            if (k2 < q) { P.mdp[sp + k2] = run + before + inc; P.dpos[sp + k2] = val; }
-            run += total;
-            __syncthreads();
         }
-        int32_t* out = P.pool + P.tail + P.off[a];
-        for (long long j = t; j < p; j += PLAN_THREADS) {
-            const int32_t y = I[j];
-            const long long ubo = ub_fence(O, len, fence, nf, fs, y);
-            const long long ubd = dsm ? ub_span(dval, q, y) : ub_span(Dg, q, y);
-            const long long del = ubd > 0 ? P.mdp[sp + ubd - 1] : 0;
-            out[j + ubo - del] = y;
-        }
-        __syncthreads();
-        for (long long k2 = t; k2 < q; k2 += PLAN_THREADS) {
-            const long long v = P.dpos[sp + k2];
-            if (v & 1) O[v >> 1] = -1;
-        }
-        const long long nl = len + p - run;
-        if (t == 0) {
-            P.row[P.aff[a]] = Row{P.tail + P.off[a], (int)nl, (int)(len + p)};
-            nnz_delta += nl - len;
-            bytes += 4 * (len + nl) + 8 * (p + q) + 16;
-        }
-        __syncthreads();
-    }
-    if (t == 0 && (nnz_delta || bytes)) {
-        atomicAdd((unsigned long long*)&P.ctr->nnz_delta, (unsigned long long)nnz_delta);
-        atomicAdd((unsigned long long*)&P.ctr->update_bytes, (unsigned long long)bytes);
     }
 }
 
-// One warp per slice of SLICE old-row entries: streams the tombstoned entries into the new
-// row. The survivors before the slice are its start minus the matched deletions before it
-// (one search in the non-decreasing dpos); survivor x lands at (#survivors before it) +
-// (#insertions < x), the insertion count searched only inside the range spanned by the
-// chunk's values, which is almost always empty. Four coalesced loads per lane per chunk.
+// Long rows: one warp per slice of SLICE old-row entries. The survivors before the slice are
+// its start minus the matched deletions before it (one search in the non-decreasing dpos);
+// survivor x lands at (#survivors before it) + (#insertions < x), the insertion count
+// searched only inside the range spanned by the chunk's values. Four coalesced loads per
+// lane per chunk.
 __global__ void k_merge_slices(int32_t* __restrict__ pool, const unsigned long long* __restrict__ keys, int B,
                                const DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg,
                                const Row* __restrict__ old_row, const int64_t* __restrict__ off, long long tail,
-                               const long long* __restrict__ mdp, const long long* __restrict__ dpos,
+                               const long long* __restrict__ E, const long long* __restrict__ dpos,
                                const int64_t* __restrict__ slices, int64_t slice_cap) {
     constexpr int U = 4;
     const long long nsl = min((long long)ctr->n_slices, (long long)slice_cap);
@@ -436,7 +483,7 @@ __global__ void k_merge_slices(int32_t* __restrict__ pool, const unsigned long l
         if (q > 0 && s0 > 0 && lane_id() == 0) {
             long long lo = 0, hi = q;
             while (lo < hi) { long long mid = (lo + hi) >> 1; if ((dpos[sp + mid] >> 1) < s0) lo = mid + 1; else hi = mid; }
-            md = lo > 0 ? mdp[sp + lo - 1] : 0;
+            md = E[sp + lo] - E[sp];
         }
         long long run = s0 - __shfl_sync(0xffffffffu, md, 0);
         const int32_t* O = pool + r.start;
@@ -487,32 +534,80 @@ __global__ void k_row_lens(const Row* __restrict__ row, int64_t n, int64_t* __re
         out[v] = row[v].len;
 }
 
-// One block per COPY_TILE entries of the compacted pool: the rows overlapping the block's
-// output range are found with one search of the new offsets, and each warp copies the
-// overlap of one row at a time, so a hub row is spread over many blocks.
-constexpr int COPY_TILE = 16384;
-__global__ void k_copy_rows(const Row* __restrict__ row, const int32_t* __restrict__ src, int32_t* __restrict__ dst,
-                            const int64_t* __restrict__ off, int32_t n, long long live) {
-    __shared__ int s_r0, s_r1;
-    const int nw = blockDim.x / WARP, w = threadIdx.x / WARP;
-    for (long long o0 = (long long)blockIdx.x * COPY_TILE; o0 < live; o0 += (long long)gridDim.x * COPY_TILE) {
-        const long long o1 = min(live, o0 + COPY_TILE);
-        if (threadIdx.x == 0) {
-            // first row with off[r + 1] > o0, last row with off[r] < o1
-            long long lo = 0, hi = n;
-            while (lo < hi) { long long mid = (lo + hi) >> 1; if (off[mid + 1] <= o0) lo = mid + 1; else hi = mid; }
-            s_r0 = (int)lo;
-            lo = 0; hi = n;
-            while (lo < hi) { long long mid = (lo + hi) >> 1; if (off[mid] < o1) lo = mid + 1; else hi = mid; }
-            s_r1 = (int)lo;   // one past the last overlapping row
+// Merge-path tiles: row r costs one unit and each of its entries one more, so row r starts
+// at unit r + off[r] and entry e of row r sits at unit r + 1 + e. One block copies the
+// entries of COPY_UNITS units: at most COPY_UNITS + 1 rows and COPY_UNITS entries, whatever
+// mix of hubs, short rows and empty rows the range holds. The rows are found with a warp
+// search and indexed in shared memory (output and source begin per row); every thread then
+// copies COPY_UNITS / COPY_THREADS entries, finding each entry's row by a search of the
+// index, with all its loads in flight before the stores.
+constexpr int COPY_UNITS = 2048;
+constexpr int COPY_THREADS = 256;
+
+// first r in [0, n) with r + off[r] > x (n if none), 32 probes per step (all lanes call)
+__device__ __forceinline__ long long warp_first_unit_above(const int64_t* off, long long n, long long x) {
+    long long lo = 0, hi = n;
+    while (hi - lo > WARP) {
+        const long long step = (hi - lo + WARP - 1) / WARP;
+        const long long pos = lo + (long long)lane_id() * step;
+        const bool le = pos < hi && pos + off[pos] <= x;
+        const int c = __popc(__ballot_sync(0xffffffffu, le));
+        const long long nlo = c == 0 ? lo : lo + (long long)(c - 1) * step + 1;
+        const long long nhi = c == 0 ? lo : min(hi, lo + (long long)c * step);
+        lo = nlo;
+        hi = max(nlo, nhi);
+        if (c == 0) break;
+    }
+    const long long pos = lo + lane_id();
+    const bool le = pos < hi && pos + off[pos] <= x;
+    return lo + __popc(__ballot_sync(0xffffffffu, le));
+}
+
+__global__ void __launch_bounds__(COPY_THREADS) k_copy_rows(const Row* __restrict__ row, const int32_t* __restrict__ src,
+                                                            int32_t* __restrict__ dst, const int64_t* __restrict__ off,
+                                                            int32_t n, long long live) {
+    __shared__ long long s_ra, s_rb;
+    __shared__ int s_ob[COPY_UNITS + 2];
+    __shared__ long long s_sb[COPY_UNITS + 2];
+    const long long units = (long long)n + live;
+    for (long long d0 = (long long)blockIdx.x * COPY_UNITS; d0 < units; d0 += (long long)gridDim.x * COPY_UNITS) {
+        const long long d1 = min(units, d0 + COPY_UNITS);
+        if (threadIdx.x < WARP) {
+            const long long ra = warp_first_unit_above(off, n, d0) - 1;       // last row starting at or before d0
+            const long long rb = warp_first_unit_above(off, n, d1 - 1) - 1;   // last row starting before d1
+            if (threadIdx.x == 0) { s_ra = ra; s_rb = rb; }
         }
         __syncthreads();
-        const int r0 = s_r0, r1 = s_r1;
-        for (int r = r0 + w; r < r1; r += nw) {
+        const long long ra = s_ra;
+        const int nr = (int)(s_rb - ra + 1);
+        const long long ef = max((long long)off[ra], d0 - ra - 1);            // first entry of the tile
+        long long el = min((long long)off[s_rb + 1], d1 - s_rb - 1);          // one past the last
+        if (el < ef) el = ef;
+        for (int i = threadIdx.x; i < nr; i += COPY_THREADS) {
+            const long long r = ra + i;
             const long long b = off[r];
-            const long long a0 = max(b, o0), a1 = min((long long)off[r + 1], o1);
-            const int32_t* sr = src + row[r].start - b;
-            for (long long i = a0 + lane_id(); i < a1; i += WARP) dst[i] = sr[i];
+            const long long eb = max(b, d0 - r - 1);
+            s_ob[i] = (int)(min(eb, el) - ef);
+            s_sb[i] = row[r].start + (eb - b);
+        }
+        __syncthreads();
+        const int span = (int)(el - ef);
+        constexpr int U = COPY_UNITS / COPY_THREADS;
+        int32_t v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int rel = threadIdx.x + u * COPY_THREADS;
+            v[u] = 0;
+            if (rel < span) {
+                int lo = 0, hi = nr - 1;   // last row whose output begin is <= rel
+                while (lo < hi) { const int mid = (lo + hi + 1) >> 1; if (s_ob[mid] <= rel) lo = mid; else hi = mid - 1; }
+                v[u] = src[s_sb[lo] + (rel - s_ob[lo])];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int rel = threadIdx.x + u * COPY_THREADS;
+            if (rel < span) dst[ef + rel] = v[u];
         }
         __syncthreads();
     }
@@ -544,8 +639,8 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     const int64_t H = 2 * M;
     size_t sz[] = {
         (size_t)M * sizeof(scout_edge), (size_t)M, (size_t)M,
-        (size_t)H * 8, (size_t)H * 8, (size_t)H * 8,
-        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)H * 4, (size_t)H * sizeof(Row)};
+        (size_t)H * 8, (size_t)H * 8, (size_t)(H + 1) * 8,
+        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)(H + 1) * 8, (size_t)H * sizeof(Row)};
     size_t total = 0;
     for (size_t s : sz) total += align256(s);
     if (c->ws) dev_free(c, c->ws, (size_t)c->ws_bytes);
@@ -566,7 +661,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     c->d_aff_seg = (int64_t*)take(sz[7]);
     c->d_aff_len = (int64_t*)take(sz[8]);
     c->d_aff_small = (int32_t*)take(sz[9]);
-    c->d_aff_large = (int32_t*)take(sz[10]);
+    c->d_small_off = (int64_t*)take(sz[10]);
     c->d_old_row = (Row*)take(sz[11]);
     c->d_hkeys = c->d_keys;
     return SCOUT_OK;
@@ -644,9 +739,9 @@ int graph_compact(scout_ctx* c, int64_t min_free, bool nnz_exact) {
         if (c->spare) { dev_free(c, c->spare, (size_t)c->spare_cap * 4); c->spare = nullptr; c->spare_cap = 0; }
         SCOUT_RC(dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool"));
     }
-    const int64_t tiles = (live + COPY_TILE - 1) / COPY_TILE;
-    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 16 * c->sm_count)), 256, 0, c->s_main>>>(
-        c->row, c->pool, np, off, (int32_t)n, (long long)live);
+    const int64_t tiles = (n + live + COPY_UNITS - 1) / COPY_UNITS;
+    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 32 * c->sm_count)), COPY_THREADS, 0,
+                  c->s_main>>>(c->row, c->pool, np, off, (int32_t)n, (long long)live);
     k_rows_compacted<<<nb, 256, 0, c->s_main>>>(c->row, off, (int32_t)n);
     SCOUT_LAUNCH(c, "compaction");
     c->nlaunch += 6;
@@ -748,10 +843,11 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_LAUNCH(c, "segments");
     c->nlaunch += 2;
     SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
-    // merge slices: sum over affected rows of max(1, ceil(len / SLICE)) <= nnz / SLICE + Amax
+    // merge slices: the long rows' ceil(len / SLICE) sum to at most nnz / SLICE + Amax
     SCOUT_RC(dev_grow(c, &c->d_slices, &c->cap_slices, c->nnz / SLICE + Amax + 1024, "merge slices"));
+    SCOUT_CU(c, cudaMemsetAsync(c->d_small_off, 0, (size_t)(Amax + 1) * 8, c->s_main));
     k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_old_row,
-                                                              c->d_aff_len, c->d_aff_small, c->d_aff_large, c->d_slices,
+                                                              c->d_aff_len, c->d_aff_small, c->d_small_off, c->d_slices,
                                                               c->cap_slices);
     SCOUT_LAUNCH(c, "k_row_alloc");
     c->nlaunch += 1;
@@ -759,19 +855,26 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     // row a starts at tail + off[a]; the total is this batch's pool growth.
     SCOUT_RC(scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems));
     long long* dpos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
-    PlanArgs pa{c->pool, c->row, c->d_old_row, sorted, B, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_aff_len,
-                (long long)c->tail, c->d_mdp, dpos, c->d_aff_small};
-    k_row_plan_warp<<<blocks_for(Amax * WARP, 256), 256, 0, c->s_main>>>(pa);
-    pa.list = c->d_aff_large;
-    k_row_plan_block<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(Amax, 2 * c->sm_count)), PLAN_THREADS, 0,
-                       c->s_main>>>(pa);
-    SCOUT_LAUNCH(c, "row plan");
-    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + Amax + 1024) * WARP, 256), 256, 0,
+    long long* E = c->d_mdp;   // matched flags, then their exclusive scan (H + 1 entries)
+    k_plan_match<<<blocks_for(H, 256), 256, 0, c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->aux_w, c->d_aff_seg,
+                                                            c->d_old_row, dpos, E, (long long)H);
+    SCOUT_LAUNCH(c, "k_plan_match");
+    SCOUT_CU(c, cudaMemsetAsync(E + H, 0, sizeof(long long), c->s_main));
+    SCOUT_RC(scan_i64(c, (int64_t*)E, H + 1, nullptr));
+    k_plan_place<<<blocks_for(H, 256), 256, 0, c->s_main>>>(c->pool, c->row, sorted, B, c->d_ctr, c->aux_w,
+                                                            c->d_aff_seg, c->d_old_row, c->d_aff_len,
+                                                            (long long)c->tail, dpos, E);
+    SCOUT_LAUNCH(c, "k_plan_place");
+    SCOUT_RC(scan_i64(c, c->d_small_off, Amax + 1, nullptr));
+    const int64_t groups = std::min<int64_t>(c->nnz, Amax * (int64_t)SMALL_LEN) / UNIT + 1;
+    k_merge_small<<<blocks_for(groups * WARP, MERGE_THREADS), MERGE_THREADS, 0, c->s_main>>>(
+        c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, (long long)c->tail, c->d_aff_small,
+        c->d_small_off);
+    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, 256), 256, 0,
                      c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len,
-                                  (long long)c->tail, c->d_mdp, dpos, c->d_slices, c->cap_slices);
-    c->nlaunch += 3;
+                                  (long long)c->tail, E, dpos, c->d_slices, c->cap_slices);
     SCOUT_LAUNCH(c, "merge");
-    c->nlaunch += 2;
+    c->nlaunch += 5;
     return SCOUT_OK;
 }
 
@@ -985,8 +1088,9 @@ int scout_graph_download(scout_ctx* c, int64_t* off, int32_t* adj, int64_t cap) 
     int32_t* tmp = nullptr;
     rc = dev_alloc(c, (void**)&tmp, (size_t)std::max<int64_t>(total, 1) * 4, "download buffer");
     if (rc != SCOUT_OK) { dev_free(c, d_off, (size_t)(n + 1) * 8); return rc; }
-    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((total + COPY_TILE - 1) / COPY_TILE, 16 * c->sm_count)),
-                  256, 0, c->s_main>>>(c->row, c->pool, tmp, d_off, (int32_t)n, (long long)total);
+    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n + total + COPY_UNITS - 1) / COPY_UNITS,
+                                                                    32 * c->sm_count)),
+                  COPY_THREADS, 0, c->s_main>>>(c->row, c->pool, tmp, d_off, (int32_t)n, (long long)total);
     cudaMemcpyAsync(adj, tmp, (size_t)total * 4, cudaMemcpyDeviceToHost, c->s_main);
     cudaError_t e = cudaStreamSynchronize(c->s_main);
     dev_free(c, tmp, (size_t)std::max<int64_t>(total, 1) * 4);

@@ -118,43 +118,50 @@ __global__ void __launch_bounds__(MIS_THREADS) k_mis(MisParams p) {
         const int nxt = cur ^ 1;
         if (leader) p.ctr->list_count[nxt] = 0;
         if (!grid_sync(p.bar, 23)) return;
-        // st_done: == epoch marks a vertex dropped in step 1 (still undecided), == DONE a vertex
-        // decided in these rounds.
-        const int32_t DONE = p.epoch + 0x40000000;
+        // st_done: == epoch marks a vertex dropped in step 1 (still undecided); DONE_IN / DONE_OUT
+        // a vertex decided in these rounds. The decision and its value live in one word, so a
+        // neighbour read once is either undecided or decided with its final membership (a
+        // separate flag read after the set entry could pair a new flag with a stale entry).
+        const int32_t DONE_IN = p.epoch + 0x40000000, DONE_OUT = p.epoch + 0x20000000;
         for (int i = wid; i < cnt; i += W) {
             int32_t c = p.list[cur][i];
             Row r = p.g.row[c];
             const int32_t* rw = p.g.pool + r.start;
+            const bool was_in = ld_volatile(p.mis + c) != 0;
             bool member_nb = false, lower_undecided = false;
-            if (ld_volatile(p.mis + c)) {
-                member_nb = true;   // already in the set: nothing to decide
-            } else {
+            if (!was_in) {
                 for (int b0 = 0; b0 < r.len && !member_nb; b0 += WARP) {
                     int k = b0 + (int)lane_id();
                     bool m = false, l = false;
                     if (k < r.len) {
                         int32_t w = rw[k];
-                        m = ld_volatile(p.mis + w) != 0;
-                        l = w < c && ld_volatile(p.st_cand + w) == p.epoch &&
-                            ld_volatile(p.st_done + w) != DONE;
+                        const int32_t sd = ld_volatile(p.st_done + w);
+                        if (sd == DONE_IN) {
+                            m = true;
+                        } else if (sd != DONE_OUT) {
+                            m = ld_volatile(p.mis + w) != 0;
+                            l = w < c && ld_volatile(p.st_cand + w) == p.epoch;
+                        }
                     }
                     member_nb = __any_sync(0xffffffffu, m);
                     lower_undecided = lower_undecided || __any_sync(0xffffffffu, l);
                     if (k < r.len) bytes += 8;
                 }
             }
+            const bool joined = !was_in && !member_nb && !lower_undecided;
             if (lane_id() == 0) {
-                if (member_nb) {
-                    p.st_done[c] = DONE;   // decided: out (or already in)
-                } else if (!lower_undecided) {
-                    p.mis[c] = 1;                                    // decided: in
-                    p.st_done[c] = DONE;
+                if (was_in) {
+                    p.st_done[c] = DONE_IN;    // kept
+                } else if (member_nb) {
+                    p.st_done[c] = DONE_OUT;
+                } else if (joined) {
+                    p.mis[c] = 1;
+                    p.st_done[c] = DONE_IN;
                 } else {
                     p.list[nxt][atomicAdd(&p.ctr->list_count[nxt], 1)] = c;   // wait
                 }
             }
-            bool joined = lane_id() == 0 && !member_nb && !lower_undecided;
-            mis_touch(p, joined, c);
+            mis_touch(p, lane_id() == 0 && joined, c);
         }
         rounds++;
         if (!grid_sync(p.bar, 24)) return;
