@@ -95,7 +95,9 @@ typedef struct scout_batch_stats {
     int64_t launches;     /* kernels launched by the call                             */
     double  ms_h2d;       /* device: copy of the edits into HBM                       */
     double  phase_ms[4];  /* device: duration of the repair kernel's first four phases   */
-    int64_t reserved[1];
+    int64_t variant;      /* repair variant that ran (BFS: 0 incremental, 1 top-down
+                             traversal, 2 direction-optimizing traversal; CC: 0
+                             incremental, 1 recompute of every class; others 0)     */
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;
@@ -175,6 +177,49 @@ int scout_commit(scout_ctx* ctx, int problem, int32_t* host_mirror, int64_t n,
  * min-id components (full_recompute_cc_gpu, scout_cc.cu:118-278). */
 int scout_recompute_bfs(scout_ctx* ctx, int32_t source, scout_batch_stats* stats);
 int scout_recompute_cc(scout_ctx* ctx, scout_batch_stats* stats);
+/* ---- learned scheduler ------------------------------------------------------------------ */
+/* No counterpart in the reference, which fixes its BFS/CC strategy with constants
+ * (scout_bfs.cu:475-476, scout_cc.cu:68-69 and 469, core/local_repair.h:13-26). BFS and CC
+ * batches can run one of several exact repair variants (scout_batch_stats.variant); with
+ * sched->policy = SCOUT_SCHED_LEARNED and a model installed for the problem, a cost model
+ * evaluated on the device between the merge and the repair picks the variant with the
+ * lowest predicted repair time. Without a model the plain policy (incremental) runs. */
+#define SCOUT_SCHED_FEATURES 24
+#define SCOUT_SCHED_OUTPUTS  4
+#define SCOUT_MLP_PARAMS     6020
+/* Installs (params != NULL, 6020 fp32 values in the layout of scout_mlp_get_params, stored
+ * as bf16 on the device) or removes (params == NULL) the model of a problem. */
+int scout_sched_install(scout_ctx* ctx, int problem, const float* params, int64_t count);
+/* Features (24), model outputs (4; NaN without a model) and decision of the last repair that
+ * ran the scheduler. */
+int scout_sched_last(scout_ctx* ctx, float* features, float* pred, int32_t* decision);
+/* Training-data probe: one batch is merged once, then every repair variant of the problem
+ * runs from the same pre-repair state and is timed (variant_ms[v] in ms, -1 for variants
+ * the problem lacks); their results must agree vertex for vertex (SCOUT_E_STATE otherwise).
+ * The batch ends in the incremental variant's state, ready for scout_commit; features
+ * receives the 24 scheduler features of the batch. */
+int scout_repair_probe(scout_ctx* ctx, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                       const scout_sched* sched, double* variant_ms, float* features,
+                       scout_batch_stats* stats);
+
+/* The cost model's own training on the device: a 24-64-64-4 ReLU perceptron with fp32
+ * master parameters, trained by hand-written forward/backward kernels and Adam, minibatch
+ * loop captured in a CUDA graph; bf16 copy for inference. Errors: scout_last_error(NULL). */
+typedef struct scout_mlp scout_mlp;
+int scout_mlp_create(int device, uint64_t seed, scout_mlp** out);
+int scout_mlp_destroy(scout_mlp* m);
+int scout_mlp_get_params(scout_mlp* m, float* out, int64_t count);
+int scout_mlp_set_params(scout_mlp* m, const float* in, int64_t count);
+/* y[n][4] = model(x[n][24]) with the fp32 parameters, or the bf16 copy when use_bf16. */
+int scout_mlp_forward(scout_mlp* m, const float* x, int64_t n, int use_bf16, float* y);
+/* Masked mean squared error over all n samples and its gradient (6020 values). */
+int scout_mlp_loss_grad(scout_mlp* m, const float* x, const float* t, const float* mask, int64_t n,
+                        float* loss, float* grad);
+/* epochs of minibatch Adam (learning rate lr) over a seeded shuffle; loss_per_epoch (may be
+ * NULL) receives the epoch's mean masked loss measured during the epoch. */
+int scout_mlp_train(scout_mlp* m, const float* x, const float* t, const float* mask, int64_t n, int epochs,
+                    int batch, float lr, uint64_t seed, float* loss_per_epoch);
+
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 

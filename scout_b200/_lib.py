@@ -39,7 +39,7 @@ class ScoutBatchStats(C.Structure):
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("ms_update", C.c_double),
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
                 ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
-                ("phase_ms", C.c_double * 4), ("reserved", C.c_int64 * 1)]
+                ("phase_ms", C.c_double * 4), ("variant", C.c_int64)]
 
     def as_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("reserved", "phase_ms")}
@@ -52,6 +52,8 @@ _i32p = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
 _u8p = C.POINTER(C.c_uint8)
 _edgep = C.POINTER(ScoutEdge)
+_f32p = C.POINTER(C.c_float)
+_f64p = C.POINTER(C.c_double)
 
 # (name, restype, argtypes) for every symbol the two headers declare.
 SIGNATURES = [
@@ -85,6 +87,17 @@ SIGNATURES = [
     ("scout_sync", C.c_int, [_vp, C.c_int64]),
     ("scout_host_alloc", C.c_int, [C.c_uint64, C.POINTER(_vp)]),
     ("scout_host_free", C.c_int, [_vp]),
+    ("scout_sched_install", C.c_int, [_vp, C.c_int, _f32p, C.c_int64]),
+    ("scout_sched_last", C.c_int, [_vp, _f32p, _f32p, _i32p]),
+    ("scout_repair_probe", C.c_int, [_vp, C.c_int, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), _f64p, _f32p,
+                                     C.POINTER(ScoutBatchStats)]),
+    ("scout_mlp_create", C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    ("scout_mlp_destroy", C.c_int, [_vp]),
+    ("scout_mlp_get_params", C.c_int, [_vp, _f32p, C.c_int64]),
+    ("scout_mlp_set_params", C.c_int, [_vp, _f32p, C.c_int64]),
+    ("scout_mlp_forward", C.c_int, [_vp, _f32p, C.c_int64, C.c_int, _f32p]),
+    ("scout_mlp_loss_grad", C.c_int, [_vp, _f32p, _f32p, _f32p, C.c_int64, _f32p, _f32p]),
+    ("scout_mlp_train", C.c_int, [_vp, _f32p, _f32p, _f32p, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, _f32p]),
     ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h
     ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),

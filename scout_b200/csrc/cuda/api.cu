@@ -69,9 +69,10 @@ static void release(scout_ctx* c) {
     cudaSetDevice(c->device);
     if (c->s_main) cudaStreamSynchronize(c->s_main);
     for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
+    sched_release(c);
     void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c, c->stamp_d,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
-                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
+                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->bfs_lv, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
                     c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
     for (void* p : devs) if (p) cudaFree(p);
     void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
@@ -236,44 +237,38 @@ int scout_set_source(scout_ctx* c, int32_t s) {
     return SCOUT_OK;
 }
 
+}  // extern "C"
+
 // ---- repair ------------------------------------------------------------------------------
-int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
-                 const scout_sched* sched, scout_batch_stats* st) {
-    if (!c || m < 0 || (m > 0 && !edits)) return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
-    if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
-    int32_t** slot = state_slot(c, problem);
-    if (!slot) return c->fail(SCOUT_E_INVALID, "unknown problem");
-    if (!*slot) return c->fail(SCOUT_E_STATE, "no state uploaded for this problem");
-    cudaSetDevice(c->device);
-    auto t0 = std::chrono::steady_clock::now();
-    scout_batch_stats local;
-    if (!st) st = &local;
-    std::memset(st, 0, sizeof(*st));
-    scout_sched sd;
-    std::memset(&sd, 0, sizeof(sd));
-    if (sched) sd = *sched;
-    c->last_problem = problem;
-    const int64_t launch0 = c->nlaunch;
-    SCOUT_RC(batch_begin(c));
-    SCOUT_RC(lists_ensure(c));
-    c->epoch++;
-    SCOUT_CU(c, cudaEventRecord(c->ev_t[0], c->s_main));
-    SCOUT_RC(graph_update(c, edits, ops, m, st));
-    SCOUT_CU(c, cudaEventRecord(c->ev_t[1], c->s_main));
-    int rc = SCOUT_OK;
+namespace scout {
+
+// Repair variant a plain (non-learned) schedule asks for: BFS 0 incremental, 1 top-down
+// traversal, 2 direction-optimizing traversal; CC 0 incremental, 1 recompute.
+static int plain_variant(int problem, const scout_sched& sd) {
+    if (sd.mode != SCOUT_MODE_RECOMPUTE) return 0;
+    if (problem == SCOUT_BFS) return sd.frontier == SCOUT_FRONTIER_QUEUE ? BFS_MODE_TOP_DOWN : BFS_MODE_DIRECTION_OPT;
+    if (problem == SCOUT_CC) return 1;
+    return 0;
+}
+
+static int run_repair(scout_ctx* c, int problem, const scout_sched& sd, int variant, const int* mode_dev,
+                      scout_batch_stats* st) {
     switch (problem) {
-    case SCOUT_BFS: rc = bfs_repair(c, st); break;
-    case SCOUT_CC: rc = cc_repair(c, &sd, st); break;
-    case SCOUT_COLORING: rc = coloring_repair(c, st); break;
-    case SCOUT_MIS: rc = mis_repair(c, st); break;
+    case SCOUT_BFS: return bfs_repair(c, variant, mode_dev, st);
+    case SCOUT_CC: {
+        scout_sched v = sd;
+        v.mode = variant ? SCOUT_MODE_RECOMPUTE : SCOUT_MODE_INCREMENTAL;
+        return cc_repair(c, &v, mode_dev, st);
     }
-    if (rc != SCOUT_OK) return rc;
-    SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
-    SCOUT_RC(counters_fetch(c));
+    case SCOUT_COLORING: return coloring_repair(c, st);
+    case SCOUT_MIS: return mis_repair(c, st);
+    }
+    return c->fail(SCOUT_E_INVALID, "unknown problem");
+}
+
+// Batch statistics from the counters of the last repair run (already fetched).
+static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
     const DevCounters& h = *c->h_ctr;
-    c->tail += h.new_elems;
-    c->nnz += h.nnz_delta;
-    c->qtag += (uint32_t)h.rounds + 8;
     st->edits = h.n_ins + h.n_del;
     st->insertions = h.n_ins;
     st->deletions = h.n_del;
@@ -295,8 +290,140 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
         unsigned long long a = h.phase_ns[i], b = h.phase_ns[i + 1];
         st->phase_ms[i] = (a && b && b >= a) ? (double)(b - a) / 1e6 : 0.0;
     }
-    st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
     c->last_changed = h.changed;
+}
+
+// Common prologue of a batch: validation, counters, classification + merge of the edits.
+static int batch_prologue(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                          scout_batch_stats* st) {
+    if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
+    int32_t** slot = state_slot(c, problem);
+    if (!slot) return c->fail(SCOUT_E_INVALID, "unknown problem");
+    if (!*slot) return c->fail(SCOUT_E_STATE, "no state uploaded for this problem");
+    cudaSetDevice(c->device);
+    std::memset(st, 0, sizeof(*st));
+    c->last_problem = problem;
+    SCOUT_RC(batch_begin(c));
+    SCOUT_RC(lists_ensure(c));
+    c->epoch++;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[0], c->s_main));
+    SCOUT_RC(graph_update(c, edits, ops, m, st));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[1], c->s_main));
+    return SCOUT_OK;
+}
+
+__global__ void k_count_diff(const int32_t* __restrict__ a, const int32_t* __restrict__ b, int64_t n,
+                             unsigned long long* __restrict__ cnt) {
+    unsigned long long d = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        d += a[v] != b[v];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(cnt, d);
+}
+
+}  // namespace scout
+
+extern "C" {
+
+int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                 const scout_sched* sched, scout_batch_stats* st) {
+    if (!c || m < 0 || (m > 0 && !edits)) return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
+    auto t0 = std::chrono::steady_clock::now();
+    scout_batch_stats local;
+    if (!st) st = &local;
+    scout_sched sd;
+    std::memset(&sd, 0, sizeof(sd));
+    if (sched) sd = *sched;
+    const int64_t launch0 = c->nlaunch;
+    SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
+    const int* mode_dev = nullptr;
+    const int variant = plain_variant(problem, sd);
+    if (sd.policy == SCOUT_SCHED_LEARNED && sched_variants(problem) > 1)
+        SCOUT_RC(sched_decide(c, problem, m, true, &mode_dev));
+    SCOUT_RC(run_repair(c, problem, sd, variant, mode_dev, st));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
+    SCOUT_RC(counters_fetch(c));
+    const DevCounters& h = *c->h_ctr;
+    c->tail += h.new_elems;
+    c->nnz += h.nnz_delta;
+    c->qtag += (uint32_t)h.rounds + 8;
+    fill_stats(c, st, launch0);
+    st->variant = mode_dev ? h.decision : variant;
+    st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
+    c->prev_repair_ms[problem] = st->ms_repair;
+    st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return SCOUT_OK;
+}
+
+int scout_repair_probe(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                       const scout_sched* sched, double* variant_ms, float* features, scout_batch_stats* st) {
+    if (!c || m < 0 || (m > 0 && !edits) || !variant_ms)
+        return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
+    const int nv = sched_variants(problem);
+    if (nv < 2) return c->fail(SCOUT_E_INVALID, "the probe applies to BFS and CC only");
+    auto t0 = std::chrono::steady_clock::now();
+    scout_batch_stats local;
+    if (!st) st = &local;
+    scout_sched sd;
+    std::memset(&sd, 0, sizeof(sd));
+    if (sched) sd = *sched;
+    const int64_t launch0 = c->nlaunch;
+    SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
+    const int* unused = nullptr;
+    SCOUT_RC(sched_decide(c, problem, m, false, &unused));
+    const int64_t n = c->n;
+    if (!c->probe_buf) SCOUT_RC(dev_alloc(c, (void**)&c->probe_buf, (size_t)(2 * n + 64) * 4, "probe buffers"));
+    if (!c->d_ctr_snap) SCOUT_RC(dev_alloc(c, (void**)&c->d_ctr_snap, sizeof(DevCounters), "probe counters"));
+    int32_t* state = *state_slot(c, problem);
+    int32_t* pre = c->probe_buf;
+    int32_t* ref = c->probe_buf + n;
+    unsigned long long* d_diff = (unsigned long long*)(c->probe_buf + 2 * n);
+    SCOUT_CU(c, cudaMemcpyAsync(c->d_ctr_snap, c->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToDevice, c->s_main));
+    SCOUT_CU(c, cudaMemcpyAsync(pre, state, (size_t)n * 4, cudaMemcpyDeviceToDevice, c->s_main));
+    // variant 0 (the incremental repair) runs last, so the batch ends in its state and its
+    // touched list is the one the commit reads
+    int order[3];
+    for (int i = 0; i < nv; i++) order[i] = (i + 1) % nv;
+    double best = 1e300;
+    for (int i = 0; i < nv; i++) {
+        const int v = order[i];
+        if (i > 0) {
+            SCOUT_CU(c, cudaMemcpyAsync(c->d_ctr, c->d_ctr_snap, sizeof(DevCounters), cudaMemcpyDeviceToDevice,
+                                        c->s_main));
+            SCOUT_CU(c, cudaMemcpyAsync(state, pre, (size_t)n * 4, cudaMemcpyDeviceToDevice, c->s_main));
+            SCOUT_CU(c, cudaMemsetAsync(c->d_bar, 0, sizeof(GridBar), c->s_main));
+            c->epoch++;
+        }
+        SCOUT_CU(c, cudaEventRecord(c->ev_t[4], c->s_main));
+        SCOUT_RC(run_repair(c, problem, sd, v, nullptr, st));
+        SCOUT_CU(c, cudaEventRecord(c->ev_t[5], c->s_main));
+        SCOUT_RC(counters_fetch(c));
+        variant_ms[v] = ev_ms(c->ev_t[4], c->ev_t[5]);
+        best = std::min(best, variant_ms[v]);
+        c->qtag += (uint32_t)c->h_ctr->rounds + 8;
+        if (i == 0) {
+            SCOUT_CU(c, cudaMemcpyAsync(ref, state, (size_t)n * 4, cudaMemcpyDeviceToDevice, c->s_main));
+        } else {
+            SCOUT_CU(c, cudaMemsetAsync(d_diff, 0, 8, c->s_main));
+            k_count_diff<<<blocks_for(n, 256), 256, 0, c->s_main>>>(state, ref, n, d_diff);
+            SCOUT_LAUNCH(c, "k_count_diff");
+            unsigned long long diff = 0;
+            SCOUT_CU(c, cudaMemcpyAsync(&diff, d_diff, 8, cudaMemcpyDeviceToHost, c->s_main));
+            SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+            if (diff)
+                return c->fail(SCOUT_E_STATE, "repair variants disagree on " + std::to_string(diff) + " vertices");
+        }
+    }
+    for (int v = nv; v < 3; v++) variant_ms[v] = -1.0;
+    const DevCounters& h = *c->h_ctr;
+    c->tail += h.new_elems;
+    c->nnz += h.nnz_delta;
+    fill_stats(c, st, launch0);
+    st->variant = 0;
+    st->ms_repair = variant_ms[0];
+    if (features) for (int i = 0; i < 24; i++) features[i] = h.feat[i];
+    c->prev_repair_ms[problem] = best;
     st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return SCOUT_OK;
 }

@@ -14,6 +14,12 @@
 //   C  relax rounds: atomicMin of level + 1 over the rows of every decreased vertex.
 // All three phases run in one cooperative launch separated by a bounded grid barrier; rows
 // longer than 1024 entries are split into 1024-entry chunks so a hub spreads over warps.
+//
+// Two full traversals from the source replace the repair when the scheduler picks one
+// (mode 1: top-down with a queue frontier; mode 2: direction-optimizing, the frontier kept
+// as the level array itself and scanned bottom-up while it is large). Both write the new
+// levels into a side array; a last pass stores and lists only the levels that changed, so
+// the commit copies back the same entries whichever variant ran.
 #include "ctx.cuh"
 
 namespace scout {
@@ -39,7 +45,10 @@ struct BfsParams {
     uint32_t qtag0;
     DevCounters* ctr;
     GridBar* bar;
-    int mode;   // 0 incremental, 1 full recompute from source
+    int mode;             // 0 incremental, 1 top-down traversal, 2 direction-optimizing traversal
+    const int* mode_dev;  // when set, the mode is read here (written on the device by the scheduler)
+    int32_t* lv_new;      // n: levels of a full traversal before they are diffed into `level`
+    long long nnz_pre;    // directed entries before this batch (the batch's delta is in ctr)
 };
 
 __device__ __forceinline__ int32_t ld_level(const int32_t* p) { return ld_volatile(p); }
@@ -134,6 +143,182 @@ __device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, 
     }
 }
 
+// ---- full traversals (modes 1 and 2) ---------------------------------------------------------
+// Frontier bookkeeping rotates over three slots like the queues: list_count[s] holds the
+// vertices and aux64[s] the adjacency entries of the frontier in q[s].
+constexpr int DO_ALPHA = 14;   // top-down -> bottom-up once frontier entries > unexplored / 14
+constexpr int DO_BETA = 24;    // bottom-up -> top-down once the frontier has < n / 24 vertices
+
+// Warp-cooperative push of newly levelled vertices (each pushed by exactly one lane, so no
+// dedupe tag is needed): chunk items into q[qi], vertex and entry counts into slot qi.
+__device__ __forceinline__ void push_new(const BfsParams& p, bool pred, int32_t y, int len, int qi) {
+    int nit = pred ? max(1, (len + CHUNK - 1) / CHUNK) : 0;
+    int incl = warp_incl_scan_i(nit);
+    int tot = __shfl_sync(0xffffffffu, incl, WARP - 1);
+    if (tot == 0) return;
+    long long deg = pred ? len : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) deg += __shfl_xor_sync(0xffffffffu, deg, o);
+    const int nv = __popc(__ballot_sync(0xffffffffu, pred));
+    int base = 0;
+    if (lane_id() == WARP - 1) {
+        base = atomicAdd(&p.ctr->q_count[qi], tot);
+        atomicAdd(&p.ctr->list_count[qi], nv);
+        atomicAdd((unsigned long long*)&p.ctr->aux64[qi], (unsigned long long)deg);
+    }
+    base = __shfl_sync(0xffffffffu, base, WARP - 1);
+    long long start = (long long)base + incl - nit;
+    for (int k = 0; k < nit; k++) {
+        long long pos = start + k;
+        if (pos < p.qcap) p.q[qi][pos] = ((unsigned long long)k << 32) | (uint32_t)y;
+        else atomicExch(&p.ctr->overflow, 1);
+    }
+}
+
+// Top-down step: every entry of every frontier item claims its unlevelled neighbours.
+__device__ void td_step(const BfsParams& p, int32_t* lv, int cur, int nxt, int d, long long& bytes) {
+    const int cnt = qcount(p, cur);
+    const int W = gwarp_count();
+    for (long long gbase = (long long)gwarp_id() * WARP; gbase < cnt; gbase += (long long)W * WARP) {
+        long long idx = gbase + lane_id();
+        bool valid = idx < cnt;
+        unsigned long long item = valid ? p.q[cur][idx] : 0ull;
+        int32_t v = (int32_t)(item & 0xffffffffu);
+        int chunk = (int)(item >> 32);
+        long long s = 0;
+        int len = 0;
+        if (valid) {
+            Row r = p.g.row[v];
+            s = r.start + (long long)chunk * CHUNK;
+            len = max(0, min(CHUNK, r.len - chunk * CHUNK));
+        }
+        int incl = warp_incl_scan_i(len);
+        int total = __shfl_sync(0xffffffffu, incl, WARP - 1);
+        int excl = incl - len;
+        bytes += (long long)len * 8 + (valid ? 24 : 0);
+        for (int e0 = 0; e0 < total; e0 += WARP) {
+            int e = e0 + (int)lane_id();
+            int lo = 0, hi = WARP - 1;
+#pragma unroll
+            for (int it = 0; it < 5; it++) {
+                int mid = (lo + hi + 1) >> 1;
+                int em = __shfl_sync(0xffffffffu, excl, mid);
+                if (em <= e) lo = mid; else hi = mid - 1;
+            }
+            long long so = __shfl_sync(0xffffffffu, s, lo);
+            int eo = __shfl_sync(0xffffffffu, excl, lo);
+            bool got = false;
+            int32_t y = 0;
+            int ylen = 0;
+            if (e < total) {
+                y = p.g.pool[so + (e - eo)];
+                if (ld_volatile(lv + y) < 0) got = atomicCAS(lv + y, -1, d + 1) == -1;
+                if (got) ylen = p.g.row[y].len;
+            }
+            push_new(p, got, y, ylen, nxt);
+        }
+    }
+}
+
+// Bottom-up step: every unlevelled vertex looks for a neighbour on level d and stops at the
+// first one. Short rows are scanned by their own lane, longer ones by the whole warp.
+__device__ void bu_step(const BfsParams& p, int32_t* lv, int nxt, int d, long long& bytes) {
+    const int64_t n = p.g.n;
+    const int W = gwarp_count();
+    for (int64_t base = (int64_t)gwarp_id() * WARP; base < n; base += (int64_t)W * WARP) {
+        const int64_t v = base + lane_id();
+        bool un = v < n && ld_volatile(lv + v) < 0;
+        Row r{0, 0, 0};
+        if (un) r = p.g.row[v];
+        bool found = false;
+        const bool big = un && r.len > WARP;
+        long long scanned = un ? 4 + 16 : (v < n ? 4 : 0);
+        if (un && !big) {
+            for (int k = 0; k < r.len; k++) {
+                scanned += 8;
+                if (ld_volatile(lv + p.g.pool[r.start + k]) == d) { found = true; break; }
+            }
+        }
+        unsigned bigm = __ballot_sync(0xffffffffu, big);
+        while (bigm) {
+            const int j = __ffs(bigm) - 1;
+            bigm &= bigm - 1;
+            const long long js = __shfl_sync(0xffffffffu, r.start, j);
+            const int jl = __shfl_sync(0xffffffffu, r.len, j);
+            bool hit = false;
+            for (int b0 = 0; b0 < jl && !hit; b0 += WARP) {
+                int k = b0 + (int)lane_id();
+                bool ok = k < jl && ld_volatile(lv + p.g.pool[js + k]) == d;
+                if (k < jl) scanned += 8;
+                hit = __any_sync(0xffffffffu, ok);
+            }
+            if ((int)lane_id() == j) found = hit;
+        }
+        if (found) lv[v] = d + 1;
+        bytes += scanned;
+        push_new(p, found, (int32_t)v, found ? r.len : 0, nxt);
+    }
+}
+
+// Full traversal into lv_new, then the diff into level. Returns false when a barrier failed.
+__device__ bool full_bfs(const BfsParams& p, int mode, long long& bytes, int& rounds) {
+    int32_t* lv = p.lv_new;
+    const int64_t n = p.g.n;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    for (int64_t v = tid; v < n; v += T) lv[v] = v == p.source ? 0 : -1;
+    if (tid == 0) bytes += 4LL * n;
+    if (leader) {
+        const int len = p.g.row[p.source].len;
+        const int nit = max(1, (len + CHUNK - 1) / CHUNK);
+        for (int k = 0; k < nit; k++) p.q[0][k] = ((unsigned long long)k << 32) | (uint32_t)p.source;
+        p.ctr->q_count[0] = nit;
+        p.ctr->list_count[0] = 1;
+        p.ctr->aux64[0] = len;
+        p.ctr->q_count[1] = p.ctr->list_count[1] = 0;
+        p.ctr->q_count[2] = p.ctr->list_count[2] = 0;
+        p.ctr->aux64[1] = p.ctr->aux64[2] = 0;
+    }
+    if (!grid_sync(p.bar, 20)) return false;
+    const long long total = p.nnz_pre + ld_volatile(&p.ctr->nnz_delta);
+    long long visited = 0;
+    bool bottom_up = false;
+    int cur = 0;
+    for (int d = 0;; d++) {
+        const int nf = ld_volatile(&p.ctr->list_count[cur]);
+        if (nf == 0) break;
+        const long long mf = ld_volatile(&p.ctr->aux64[cur]);
+        visited += mf;
+        if (mode == 2) {
+            if (!bottom_up && mf > (total - visited) / DO_ALPHA) bottom_up = true;
+            else if (bottom_up && (long long)nf * DO_BETA < n) bottom_up = false;
+        }
+        const int nxt = (cur + 1) % 3, zer = (cur + 2) % 3;
+        if (leader) { p.ctr->q_count[zer] = 0; p.ctr->list_count[zer] = 0; p.ctr->aux64[zer] = 0; }
+        if (bottom_up) bu_step(p, lv, nxt, d, bytes);
+        else td_step(p, lv, cur, nxt, d, bytes);
+        rounds++;
+        if (!grid_sync(p.bar, 21)) return false;
+        cur = nxt;
+    }
+    // diff: store and list the levels that changed
+    for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
+        const int64_t v = b + lane_id();
+        bool ch = false;
+        int32_t nv = 0;
+        if (v < n) {
+            nv = lv[v];
+            ch = nv != p.level[v];
+            if (ch) p.level[v] = nv;
+        }
+        int ti = warp_append(ch, &p.ctr->changed);
+        if (ch) p.touched[ti] = (int32_t)v;
+    }
+    if (tid == 0) bytes += 12LL * n;
+    return true;
+}
+
 __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
     const int W = gwarp_count();
     const int wid = gwarp_id();
@@ -146,24 +331,21 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
     int cur = 0;
     phase_mark(&p.ctr->phase_ns[0]);
 
-    if (p.mode == 1) {
-        // Full recompute: every vertex restarts at +inf; all become touched.
-        for (int64_t v = tid; v < p.g.n; v += T) {
-            p.level[v] = v == p.source ? 0 : -1;
-            p.touched[v] = (int32_t)v;
-            p.st_touch[v] = p.epoch;
-        }
+    const int mode = p.mode_dev ? *p.mode_dev : p.mode;
+    if (mode != 0) {
+        if (!full_bfs(p, mode, bytes, rounds)) return;
+        phase_mark(&p.ctr->phase_ns[3]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
         if (leader) {
-            p.ctr->changed = p.g.n;
-            int len = p.g.row[p.source].len;
-            int nit = (len + CHUNK - 1) / CHUNK;
-            for (int k = 0; k < nit; k++) p.q[0][k] = ((unsigned long long)k << 32) | (uint32_t)p.source;
-            p.ctr->q_count[0] = nit;
-            p.st_q[p.source] = tag;
+            p.ctr->rounds = rounds;
+            p.ctr->affected = p.g.n;
+            p.ctr->recomputes = 1;
         }
-        if (tid == 0) bytes += (long long)p.g.n * 12;
-        if (!grid_sync(p.bar, 1)) return;
-    } else {
+        return;
+    }
+    {
         // ---- A: invalidation -------------------------------------------------------------
         // Candidates are queued as CHUNK-sized items of their rows. A single-chunk candidate
         // is settled by one warp (parent check, invalidation, children pushed). A longer one
@@ -396,9 +578,10 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
     }
 }
 
-static int bfs_launch(scout_ctx* c, int mode, scout_batch_stats* st) {
+static int bfs_launch(scout_ctx* c, int mode, const int* mode_dev, scout_batch_stats* st) {
     (void)st;
     SCOUT_RC(lists_ensure(c));
+    if (!c->bfs_lv) SCOUT_RC(dev_alloc(c, (void**)&c->bfs_lv, (size_t)c->n * 4, "BFS traversal levels"));
     BfsParams p;
     p.g = dgraph(c);
     p.level = c->level;
@@ -418,14 +601,19 @@ static int bfs_launch(scout_ctx* c, int mode, scout_batch_stats* st) {
     p.ctr = c->d_ctr;
     p.bar = c->d_bar;
     p.mode = mode;
+    p.mode_dev = mode_dev;
+    p.lv_new = c->bfs_lv;
+    p.nnz_pre = c->nnz;
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_bfs, BFS_THREADS, args, 0);
 }
 
-int bfs_repair(scout_ctx* c, scout_batch_stats* st) { return bfs_launch(c, 0, st); }
+int bfs_repair(scout_ctx* c, int mode, const int* mode_dev, scout_batch_stats* st) {
+    return bfs_launch(c, mode, mode_dev, st);
+}
 int bfs_recompute(scout_ctx* c, int32_t source, scout_batch_stats* st) {
     c->source = source;
-    return bfs_launch(c, 1, st);
+    return bfs_launch(c, BFS_MODE_DIRECTION_OPT, nullptr, st);
 }
 
 }  // namespace scout

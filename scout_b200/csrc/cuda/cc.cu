@@ -58,6 +58,7 @@ struct CcParams {
     int32_t epoch;
     int bound;
     int full;           // 1: recompute every class
+    const int* mode_dev;  // when set, full = (*mode_dev != 0), decided on the device by the scheduler
     DevCounters* ctr;
     GridBar* bar;
 };
@@ -254,9 +255,10 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
     const int nh = ld_volatile(&p.ctr->n_half);
     long long bytes = 0;
     __shared__ int s_task;
+    const int full = p.mode_dev ? (*p.mode_dev != 0) : p.full;
 
     phase_mark(&p.ctr->phase_ns[0]);
-    if (!p.full) {
+    if (!full) {
         // ---- P0: unions of inserted edges ---------------------------------------------------
         for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
             int64_t k = b + lane_id();
@@ -456,20 +458,16 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
             p.firstw[cls] = -1;
         }
     } else {
-        for (int64_t v = tid; v < n; v += T) {
-            p.touched[v] = (int32_t)v;
-            p.st_touch[v] = p.epoch;
-        }
-        if (leader) p.ctr->changed = (int)n;
+        // every class is recomputed; the final pass lists only the labels that change
         if (leader) p.ctr->recomputes = 1;
     }
     // ---- P3: exact recompute of dirty classes (every class when full) ------------------------
     if (!grid_sync(p.bar, 38)) return;
-    if (!p.full && ld_volatile(&p.ctr->recomputes) == 0) {
+    if (!full && ld_volatile(&p.ctr->recomputes) == 0) {
         goto done;
     }
     for (int64_t v = tid; v < n; v += T) {
-        bool d = p.full || ld_volatile(p.dirty + p.label[v]) == p.epoch;
+        bool d = full || ld_volatile(p.dirty + p.label[v]) == p.epoch;
         p.vp[v] = d ? (int32_t)v : -1;
     }
     if (!grid_sync(p.bar, 36)) return;
@@ -579,7 +577,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
             int32_t root = uf_find(p.vp, (int32_t)v);
             if (p.label[v] != root) { p.label[v] = root; ch = true; }
         }
-        if (!p.full) cc_touch(p, ch, (int32_t)v);
+        cc_touch(p, ch, (int32_t)v);
     }
     if (tid == 0) bytes += 16LL * n;
 done:
@@ -587,7 +585,7 @@ done:
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
     if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
-    if (leader) p.ctr->affected = p.ctr->changed;
+    if (leader) p.ctr->affected = full ? (int)n : p.ctr->changed;
 }
 
 __global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, int32_t* __restrict__ newmin,
@@ -600,7 +598,7 @@ __global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, i
     }
 }
 
-static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
+static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int* mode_dev) {
     SCOUT_RC(lists_ensure(c));
     const int64_t n = c->n;
     if (!c->d_cc) {   // uf, cnt, dirty, remf, newmin, vp, firstw, hcnt
@@ -643,6 +641,7 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
     int64_t bound = sched && sched->search_bound > 0 ? sched->search_bound : 5000;
     p.bound = (int)std::min<int64_t>(bound, CC_MAX_BOUND);
     p.full = full;
+    p.mode_dev = mode_dev;
     p.ctr = c->d_ctr;
     p.bar = c->d_bar;
     static bool attr = false;
@@ -654,15 +653,15 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full) {
     return coop_launch(c, (const void*)k_cc, CC_THREADS, args, CC_SMEM);
 }
 
-int cc_repair(scout_ctx* c, const scout_sched* sched, scout_batch_stats* st) {
+int cc_repair(scout_ctx* c, const scout_sched* sched, const int* mode_dev, scout_batch_stats* st) {
     (void)st;
     int full = sched && sched->mode == SCOUT_MODE_RECOMPUTE ? 1 : 0;
-    return cc_launch(c, sched, full);
+    return cc_launch(c, sched, full, mode_dev);
 }
 
 int cc_recompute(scout_ctx* c, scout_batch_stats* st) {
     (void)st;
-    return cc_launch(c, nullptr, 1);
+    return cc_launch(c, nullptr, 1, nullptr);
 }
 
 }  // namespace scout

@@ -39,6 +39,14 @@ struct DevCounters {
     long long hbm_bytes;      // algorithmic bytes of the repair
     long long aux64[4];
     unsigned long long phase_ns[8];   // %globaltimer marks written by the repair kernels
+    // scheduler: feature accumulators, the 24 features, the model's 4 outputs, its decision
+    int sched_hist[16];       // affected rows by floor(log2(1 + new degree))
+    int sched_del_hit;        // deletion half-edits meeting the problem's structural test
+    int sched_del;            // deletion half-edits
+    int decision;             // repair variant the kernels run (read on the device)
+    int sched_flags;          // 1 features computed, 2 model applied
+    float feat[24];
+    float pred[4];
 };
 
 struct scout_ctx {
@@ -116,6 +124,13 @@ struct scout_ctx {
     int64_t* d_scan_tmp = nullptr;  int64_t cap_scan = 0;
     void* d_misc = nullptr;         int64_t cap_misc = 0;   // colouring proposal markers
     int32_t* d_cc = nullptr;        // component scratch (7 n int32)
+    int32_t* bfs_lv = nullptr;      // levels of a full BFS traversal before the diff (n int32)
+
+    // ---- scheduler ----
+    void* model[4] = {nullptr, nullptr, nullptr, nullptr};   // bf16 cost model per problem
+    double prev_repair_ms[4] = {0, 0, 0, 0};                  // last batch's repair time per problem
+    int32_t* probe_buf = nullptr;   // probe: pre-repair state, first variant's result, mismatch counter
+    DevCounters* d_ctr_snap = nullptr;
 
     DevCounters* d_ctr = nullptr;
     DevCounters* h_ctr = nullptr;   // pinned
@@ -202,12 +217,22 @@ int lists_ensure(scout_ctx* c);
 int batch_begin(scout_ctx* c);   // zeroes the counters and the barrier for a new batch
 int counters_fetch(scout_ctx* c); // copies the device counters into c->h_ctr (synchronous)
 // problem kernels (their .cu files)
-int bfs_repair(scout_ctx* c, scout_batch_stats* st);
+// BFS repair variants: 0 incremental, 1 top-down traversal, 2 direction-optimizing
+// traversal; mode_dev (device int) overrides mode when the scheduler decides on the device.
+constexpr int BFS_MODE_INCREMENTAL = 0, BFS_MODE_TOP_DOWN = 1, BFS_MODE_DIRECTION_OPT = 2;
+int bfs_repair(scout_ctx* c, int mode, const int* mode_dev, scout_batch_stats* st);
 int bfs_recompute(scout_ctx* c, int32_t source, scout_batch_stats* st);
-int cc_repair(scout_ctx* c, const scout_sched* sched, scout_batch_stats* st);
+// CC repair variants: 0 incremental, 1 recompute of every class; mode_dev as for BFS.
+int cc_repair(scout_ctx* c, const scout_sched* sched, const int* mode_dev, scout_batch_stats* st);
 int cc_recompute(scout_ctx* c, scout_batch_stats* st);
 int coloring_repair(scout_ctx* c, scout_batch_stats* st);
 int mis_repair(scout_ctx* c, scout_batch_stats* st);
+// sched.cu: features + on-device inference of the installed model; writes ctr->decision.
+// Returns SCOUT_OK and sets *mode_dev to the decision's device address when the learned
+// policy applies to the problem, else leaves it null (plain policy).
+int sched_decide(scout_ctx* c, int problem, int64_t m, bool use_model, const int** mode_dev);
+void sched_release(scout_ctx* c);
+int sched_variants(int problem);   // repair variants a problem has (BFS 3, CC 2, others 1)
 // persistent launch helper
 int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem);
 

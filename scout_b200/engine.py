@@ -49,6 +49,10 @@ def _p64(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_int64))
 
 
+def _pf32(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
 def _pedge(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(ScoutEdge))
 
@@ -191,6 +195,40 @@ class Context:
         self._c(LIB.scout_repair(self._h, _prob(problem), _pedge(e), op, len(e), C.byref(sd), C.byref(st)))
         return st.as_dict()
 
+    def repair_probe(self, problem, edges, ops=None, sched: Optional[dict] = None):
+        """One batch, every repair variant timed from the same pre-repair state (results must
+        agree). Returns (stats, variant_ms[3] with -1 for absent variants, features[24])."""
+        e = as_edges(edges)
+        st = ScoutBatchStats()
+        sd = ScoutSched()
+        for k, v in (sched or {}).items():
+            setattr(sd, k, v)
+        op = None
+        if ops is not None:
+            ops = np.ascontiguousarray(ops, dtype=np.uint8)
+            op = ops.ctypes.data_as(C.POINTER(C.c_uint8))
+        ms = np.zeros(3, dtype=np.float64)
+        feat = np.zeros(24, dtype=np.float32)
+        self._c(LIB.scout_repair_probe(self._h, _prob(problem), _pedge(e), op, len(e), C.byref(sd),
+                                       ms.ctypes.data_as(C.POINTER(C.c_double)), _pf32(feat), C.byref(st)))
+        return st.as_dict(), ms, feat
+
+    def sched_install(self, problem, params) -> None:
+        """Installs a cost model (6020 fp32 parameters) for BFS or CC; None removes it."""
+        if params is None:
+            self._c(LIB.scout_sched_install(self._h, _prob(problem), None, 0))
+            return
+        w = np.ascontiguousarray(params, dtype=np.float32)
+        self._c(LIB.scout_sched_install(self._h, _prob(problem), _pf32(w), w.size))
+
+    def sched_last(self):
+        """(features[24], predictions[4], decision) of the last repair that ran the scheduler."""
+        f = np.zeros(24, dtype=np.float32)
+        y = np.zeros(4, dtype=np.float32)
+        d = C.c_int32()
+        self._c(LIB.scout_sched_last(self._h, _pf32(f), _pf32(y), C.byref(d)))
+        return f, y, d.value
+
     def commit(self, problem, mirror: np.ndarray) -> int:
         if mirror.dtype != np.int32 or not mirror.flags.c_contiguous:
             raise ValueError("mirror must be a contiguous int32 array")
@@ -210,6 +248,72 @@ class Context:
 
     def sync(self, timeout_us: int = 0) -> None:
         self._c(LIB.scout_sync(self._h, int(timeout_us)))
+
+
+class MLP:
+    """The scheduler's cost model (24-64-64-4 ReLU perceptron) on the device: fp32 master
+    parameters trained by the library's own forward/backward/Adam kernels, bf16 copy for
+    inference. Parameters are one flat vector of 6020 values (W1, b1, W2, b2, W3, b3; row j
+    of a weight matrix = input weights of unit j)."""
+
+    NPARAM = 6020
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        _check(LIB.scout_mlp_create(int(device), int(seed), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            LIB.scout_mlp_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        w = np.zeros(self.NPARAM, dtype=np.float32)
+        _check(LIB.scout_mlp_get_params(self._h, _pf32(w), self.NPARAM))
+        return w
+
+    @params.setter
+    def params(self, w) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(LIB.scout_mlp_set_params(self._h, _pf32(w), w.size))
+
+    def forward(self, x, bf16: bool = False) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 24)
+        y = np.zeros((len(x), 4), dtype=np.float32)
+        _check(LIB.scout_mlp_forward(self._h, _pf32(x), len(x), int(bf16), _pf32(y)))
+        return y
+
+    def loss_grad(self, x, t, mask):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 24)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, 4)
+        m = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1, 4)
+        loss = C.c_float()
+        g = np.zeros(self.NPARAM, dtype=np.float32)
+        _check(LIB.scout_mlp_loss_grad(self._h, _pf32(x), _pf32(t), _pf32(m), len(x), C.byref(loss), _pf32(g)))
+        return float(loss.value), g
+
+    def train(self, x, t, mask, epochs: int = 200, batch: int = 256, lr: float = 3e-3, seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 24)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, 4)
+        m = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1, 4)
+        losses = np.zeros(max(epochs, 1), dtype=np.float32)
+        _check(LIB.scout_mlp_train(self._h, _pf32(x), _pf32(t), _pf32(m), len(x), int(epochs), int(batch),
+                                   float(lr), int(seed), _pf32(losses)))
+        return losses[:epochs]
 
 
 # ---------------------------------------------------------------------------------------
