@@ -220,6 +220,39 @@ int scout_mlp_loss_grad(scout_mlp* m, const float* x, const float* t, const floa
 int scout_mlp_train(scout_mlp* m, const float* x, const float* t, const float* mask, int64_t n, int epochs,
                     int batch, float lr, uint64_t seed, float* loss_per_epoch);
 
+/* ---- batched multi-stream engine ---------------------------------------------------------- */
+/* No counterpart in the reference, which runs one update stream per process
+ * (scout_bfs.cu:517-629, scout_cc.cu:443-554, scout_coloring.cu:279-371, scout_mis.cu:769-1013).
+ * K independent streams of one problem, each with its own graph, live as a disjoint union in
+ * one device store (stream k owns the vertex range [base_k, base_k + n_k)). A round takes at
+ * most one pending batch per stream and runs their union as one batch: one merge, one
+ * persistent repair kernel whose work queues hold every stream's items, one commit. Each
+ * stream's solution equals the one it would have alone (stream-local vertex ids throughout). */
+typedef struct scout_multi scout_multi;
+int scout_multi_create(int device, int problem, uint64_t hbm_budget_bytes, scout_multi** out);
+int scout_multi_destroy(scout_multi* m);
+/* The engine's underlying context (scheduler model install, graph info, compaction). */
+scout_ctx* scout_multi_context(scout_multi* m);
+/* Adds a stream before the first round: its CSR (n vertices, off[n + 1], adj), its initial
+ * solution in the problem's layout (CC labels: vertex ids of the stream), and its BFS source;
+ * *stream_id receives its index. */
+int scout_multi_add_stream(scout_multi* m, int64_t n, const int64_t* off, const int32_t* adj, const int32_t* init,
+                           int32_t source, int32_t* stream_id);
+/* Uploads the union (also done by the first round). */
+int scout_multi_seal(scout_multi* m);
+/* One round of k batches: batch i belongs to stream stream_ids[i] (distinct), with counts[i]
+ * edits in stream-local ids and optional ops[i] (NULL array or entry: toggles). Edits whose
+ * ids fall outside their stream's graph are skipped. */
+int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched,
+                      scout_batch_stats* stats);
+/* Changed entries of the last round into per-stream host mirrors (mirrors[k]: n_k entries, or
+ * NULL to skip stream k); *changed receives the number of entries that changed. */
+int scout_multi_commit(scout_multi* m, int32_t* const* mirrors, int64_t* changed);
+/* One stream's current solution (n = the stream's vertex count). */
+int scout_multi_download(scout_multi* m, int32_t stream, int32_t* out, int64_t n);
+int scout_multi_streams(scout_multi* m, int32_t* count, int64_t* total_vertices);
+
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 

@@ -98,6 +98,16 @@ SIGNATURES = [
     ("scout_mlp_forward", C.c_int, [_vp, _f32p, C.c_int64, C.c_int, _f32p]),
     ("scout_mlp_loss_grad", C.c_int, [_vp, _f32p, _f32p, _f32p, C.c_int64, _f32p, _f32p]),
     ("scout_mlp_train", C.c_int, [_vp, _f32p, _f32p, _f32p, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, _f32p]),
+    ("scout_multi_create", C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    ("scout_multi_destroy", C.c_int, [_vp]),
+    ("scout_multi_context", _vp, [_vp]),
+    ("scout_multi_add_stream", C.c_int, [_vp, C.c_int64, _i64p, _i32p, _i32p, C.c_int32, _i32p]),
+    ("scout_multi_seal", C.c_int, [_vp]),
+    ("scout_multi_round", C.c_int, [_vp, C.c_int32, _i32p, C.POINTER(_edgep), _i64p, C.POINTER(_u8p),
+                                    C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_multi_commit", C.c_int, [_vp, C.POINTER(_i32p), _i64p]),
+    ("scout_multi_download", C.c_int, [_vp, C.c_int32, _i32p, C.c_int64]),
+    ("scout_multi_streams", C.c_int, [_vp, _i32p, _i64p]),
     ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h
     ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),

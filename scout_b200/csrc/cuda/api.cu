@@ -72,7 +72,7 @@ static void release(scout_ctx* c) {
     sched_release(c);
     void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c, c->stamp_d,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
-                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->bfs_lv, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
+                    c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->bfs_lv, c->d_sources, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
                     c->d_stage_ids[1], c->d_stage_off[0], c->d_stage_off[1]};
     for (void* p : devs) if (p) cudaFree(p);
     void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
@@ -312,6 +312,30 @@ static int batch_prologue(scout_ctx* c, int problem, const scout_edge* edits, co
     return SCOUT_OK;
 }
 
+// (id, value) pairs of the last repair's touched entries, gathered on the device and copied
+// into the context's page-locked buffer (*pairs points there until the next call).
+int commit_gather(scout_ctx* c, int problem, const int32_t** pairs, int64_t* count) {
+    int32_t** slot = state_slot(c, problem);
+    if (!slot || !*slot) return c->fail(SCOUT_E_STATE, "nothing to commit for this problem");
+    if (problem != c->last_problem) return c->fail(SCOUT_E_STATE, "the last repair was for another problem");
+    cudaSetDevice(c->device);
+    const int64_t cnt = c->last_changed;
+    *pairs = nullptr;
+    *count = 0;
+    if (cnt > 0) {
+        SCOUT_RC(pin_grow(c, &c->h_pin_commit, &c->cap_pin_commit, cnt * 8));
+        k_commit_gather<<<blocks_for(cnt, 256), 256, 0, c->s_main>>>(c->d_list[0], c->d_ctr, *slot, c->d_commit);
+        SCOUT_LAUNCH(c, "k_commit_gather");
+        c->nlaunch += 1;
+        SCOUT_CU(c, cudaMemcpyAsync(c->h_pin_commit, c->d_commit, (size_t)cnt * 8, cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        *pairs = (const int32_t*)c->h_pin_commit;
+        *count = cnt;
+    }
+    c->last_changed = 0;
+    return SCOUT_OK;
+}
+
 __global__ void k_count_diff(const int32_t* __restrict__ a, const int32_t* __restrict__ b, int64_t n,
                              unsigned long long* __restrict__ cnt) {
     unsigned long long d = 0;
@@ -435,28 +459,17 @@ int scout_repair_cc(scout_ctx* c, const scout_edge* e, const uint8_t* o, int64_t
 
 int scout_commit(scout_ctx* c, int problem, int32_t* mirror, int64_t n, int64_t* changed) {
     if (!c || !mirror) return SCOUT_E_INVALID;
-    int32_t** slot = state_slot(c, problem);
-    if (!slot || !*slot || n != c->n) return c->fail(SCOUT_E_STATE, "nothing to commit for this problem");
-    if (problem != c->last_problem) return c->fail(SCOUT_E_STATE, "the last repair was for another problem");
-    cudaSetDevice(c->device);
-    int64_t cnt = c->last_changed;
+    if (n != c->n) return c->fail(SCOUT_E_STATE, "nothing to commit for this problem");
+    const int32_t* p = nullptr;
+    int64_t cnt = 0;
+    SCOUT_RC(commit_gather(c, problem, &p, &cnt));
     int64_t diff = 0;
-    if (cnt > 0) {
-        SCOUT_RC(pin_grow(c, &c->h_pin_commit, &c->cap_pin_commit, cnt * 8));
-        k_commit_gather<<<blocks_for(cnt, 256), 256, 0, c->s_main>>>(c->d_list[0], c->d_ctr, *slot, c->d_commit);
-        SCOUT_LAUNCH(c, "k_commit_gather");
-        c->nlaunch += 1;
-        SCOUT_CU(c, cudaMemcpyAsync(c->h_pin_commit, c->d_commit, (size_t)cnt * 8, cudaMemcpyDeviceToHost, c->s_main));
-        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
-        const int32_t* p = (const int32_t*)c->h_pin_commit;
-        for (int64_t i = 0; i < cnt; i++) {
-            int32_t v = p[2 * i], x = p[2 * i + 1];
-            if (v < 0 || v >= n) continue;
-            if (mirror[v] != x) { mirror[v] = x; diff++; }
-        }
+    for (int64_t i = 0; i < cnt; i++) {
+        int32_t v = p[2 * i], x = p[2 * i + 1];
+        if (v < 0 || v >= n) continue;
+        if (mirror[v] != x) { mirror[v] = x; diff++; }
     }
     if (changed) *changed = diff;
-    c->last_changed = 0;
     return SCOUT_OK;
 }
 

@@ -49,6 +49,8 @@ struct BfsParams {
     const int* mode_dev;  // when set, the mode is read here (written on the device by the scheduler)
     int32_t* lv_new;      // n: levels of a full traversal before they are diffed into `level`
     long long nnz_pre;    // directed entries before this batch (the batch's delta is in ctr)
+    const int32_t* sources;   // when nsrc > 0: every listed vertex is a level-0 root (a union of
+    int nsrc;                 // disjoint graphs, one source each); else `source` alone
 };
 
 __device__ __forceinline__ int32_t ld_level(const int32_t* p) { return ld_volatile(p); }
@@ -267,15 +269,27 @@ __device__ bool full_bfs(const BfsParams& p, int mode, long long& bytes, int& ro
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
-    for (int64_t v = tid; v < n; v += T) lv[v] = v == p.source ? 0 : -1;
+    for (int64_t v = tid; v < n; v += T) lv[v] = -1;
     if (tid == 0) bytes += 4LL * n;
+    if (!grid_sync(p.bar, 22)) return false;
     if (leader) {
-        const int len = p.g.row[p.source].len;
-        const int nit = max(1, (len + CHUNK - 1) / CHUNK);
-        for (int k = 0; k < nit; k++) p.q[0][k] = ((unsigned long long)k << 32) | (uint32_t)p.source;
-        p.ctr->q_count[0] = nit;
-        p.ctr->list_count[0] = 1;
-        p.ctr->aux64[0] = len;
+        const int ns = p.nsrc > 0 ? p.nsrc : 1;
+        int items = 0;
+        long long deg = 0;
+        for (int i = 0; i < ns; i++) {
+            const int32_t s = p.nsrc > 0 ? p.sources[i] : p.source;
+            lv[s] = 0;
+            const int len = p.g.row[s].len;
+            const int nit = max(1, (len + CHUNK - 1) / CHUNK);
+            for (int k = 0; k < nit && items + k < p.qcap; k++)
+                p.q[0][items + k] = ((unsigned long long)k << 32) | (uint32_t)s;
+            items += nit;
+            deg += len;
+        }
+        if (items > p.qcap) { p.ctr->overflow = 1; items = (int)p.qcap; }
+        p.ctr->q_count[0] = items;
+        p.ctr->list_count[0] = ns;
+        p.ctr->aux64[0] = deg;
         p.ctr->q_count[1] = p.ctr->list_count[1] = 0;
         p.ctr->q_count[2] = p.ctr->list_count[2] = 0;
         p.ctr->aux64[1] = p.ctr->aux64[2] = 0;
@@ -604,6 +618,8 @@ static int bfs_launch(scout_ctx* c, int mode, const int* mode_dev, scout_batch_s
     p.mode_dev = mode_dev;
     p.lv_new = c->bfs_lv;
     p.nnz_pre = c->nnz;
+    p.sources = c->d_sources;
+    p.nsrc = c->nsrc;
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_bfs, BFS_THREADS, args, 0);
 }

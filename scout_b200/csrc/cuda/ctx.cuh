@@ -82,6 +82,8 @@ struct scout_ctx {
     int32_t* label = nullptr;
     int32_t* mis = nullptr;
     int32_t source = 0;
+    int32_t* d_sources = nullptr;   // BFS roots of a union of graphs (nsrc > 0), else `source`
+    int nsrc = 0;
     int last_problem = -1;
 
     // ---- persistent per-vertex scratch (stamped with a batch epoch; never cleared) ----
@@ -233,6 +235,8 @@ int mis_repair(scout_ctx* c, scout_batch_stats* st);
 int sched_decide(scout_ctx* c, int problem, int64_t m, bool use_model, const int** mode_dev);
 void sched_release(scout_ctx* c);
 int sched_variants(int problem);   // repair variants a problem has (BFS 3, CC 2, others 1)
+// api.cu: the last repair's (id, value) pairs in page-locked memory (valid until the next call)
+int commit_gather(scout_ctx* c, int problem, const int32_t** pairs, int64_t* count);
 // persistent launch helper
 int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem);
 

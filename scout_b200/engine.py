@@ -101,12 +101,22 @@ class Context:
         h = C.c_void_p()
         _check(LIB.scout_ctx_create(int(device), int(budget_bytes), C.byref(h)))
         self._h = h
+        self._own = True
         self.n = 0
 
+    @classmethod
+    def _borrow(cls, handle) -> "Context":
+        """A view of a context owned by someone else (a MultiEngine); never destroyed here."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        self._own = False
+        self.n = 0
+        return self
+
     def close(self) -> None:
-        if self._h:
+        if self._h and self._own:
             LIB.scout_ctx_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __enter__(self):
         return self
@@ -248,6 +258,105 @@ class Context:
 
     def sync(self, timeout_us: int = 0) -> None:
         self._c(LIB.scout_sync(self._h, int(timeout_us)))
+
+
+def form_rounds(arrivals, max_edits: int):
+    """Groups (stream_id, batch) arrivals into rounds for MultiEngine.round: each batch goes
+    to the earliest round after its stream's previous batch that still has room for it
+    (at most max_edits per round, a larger batch alone), so every stream keeps its order and
+    small batches of many streams share a round. Returns a list of [(stream_id, batch), ...]."""
+    rounds, totals, last = [], [], {}
+    for sid, b in arrivals:
+        r = last.get(sid, -1) + 1
+        while r < len(rounds) and totals[r] > 0 and totals[r] + len(b) > max_edits:
+            r += 1
+        while r >= len(rounds):
+            rounds.append([])
+            totals.append(0)
+        rounds[r].append((sid, b))
+        totals[r] += len(b)
+        last[sid] = r
+    return rounds
+
+
+class MultiEngine:
+    """Batched multi-stream engine: K independent streams of one problem (each with its own
+    graph and solution) kept as a disjoint union in one device store; a round runs at most
+    one batch per stream as a single batch of the union. Ids stay stream-local."""
+
+    def __init__(self, problem, device: int = 0, budget_bytes: int = 0):
+        h = C.c_void_p()
+        _check(LIB.scout_multi_create(int(device), _prob(problem), int(budget_bytes), C.byref(h)))
+        self._h = h
+        self.problem = problem
+        self.sizes = []
+
+    def close(self) -> None:
+        if self._h:
+            LIB.scout_multi_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc: int) -> None:
+        _check(rc, LIB.scout_multi_context(self._h) if self._h else None)
+
+    @property
+    def context(self) -> "Context":
+        """The underlying device context (not owned): scheduler install, graph info."""
+        return Context._borrow(LIB.scout_multi_context(self._h))
+
+    def add_stream(self, off, adj, init, source: int = 0) -> int:
+        off = _i64(off)
+        adj = _i32(adj)
+        init = _i32(init)
+        sid = C.c_int32()
+        self._c(LIB.scout_multi_add_stream(self._h, len(off) - 1, _p64(off), _p32(adj), _p32(init), int(source),
+                                           C.byref(sid)))
+        self.sizes.append(len(off) - 1)
+        return sid.value
+
+    def seal(self) -> None:
+        self._c(LIB.scout_multi_seal(self._h))
+
+    def round(self, batches, sched: Optional[dict] = None) -> dict:
+        """batches: [(stream_id, edges), ...] with distinct stream ids."""
+        k = len(batches)
+        ids = np.array([s for s, _ in batches], dtype=np.int32)
+        arrs = [as_edges(b) for _, b in batches]
+        ptrs = (C.POINTER(ScoutEdge) * max(k, 1))(*[_pedge(a) for a in arrs])
+        counts = np.array([len(a) for a in arrs], dtype=np.int64)
+        st = ScoutBatchStats()
+        sd = ScoutSched()
+        for key, v in (sched or {}).items():
+            setattr(sd, key, v)
+        self._c(LIB.scout_multi_round(self._h, k, _p32(ids), ptrs, _p64(counts), None, C.byref(sd), C.byref(st)))
+        return st.as_dict()
+
+    def commit(self, mirrors) -> int:
+        """mirrors[k]: int32 host mirror of stream k (None to skip)."""
+        for m in mirrors:
+            if m is not None and (m.dtype != np.int32 or not m.flags.c_contiguous):
+                raise ValueError("mirrors must be contiguous int32 arrays")
+        arr = (C.POINTER(C.c_int32) * len(mirrors))(*[(_p32(m) if m is not None else None) for m in mirrors])
+        ch = C.c_int64()
+        self._c(LIB.scout_multi_commit(self._h, arr, C.byref(ch)))
+        return ch.value
+
+    def download(self, sid: int) -> np.ndarray:
+        out = np.zeros(self.sizes[sid], dtype=np.int32)
+        self._c(LIB.scout_multi_download(self._h, int(sid), _p32(out), len(out)))
+        return out
 
 
 class MLP:
