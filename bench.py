@@ -55,6 +55,12 @@ def parse_args():
     ap.add_argument("--ref-timeout", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true", help="per-batch statistics on stderr")
+    ap.add_argument("--model", default=os.path.join(ROOT, "scout_b200", "sched_model.npz"),
+                    help="trained scheduler model (BFS/CC); the plain policy runs without it")
+    ap.add_argument("--tuned", default=os.path.join(ROOT, "scout_b200", "tuned.json"),
+                    help="autotuned launch knobs (python -m scout_b200.autotune); defaults without it")
+    ap.add_argument("--no-multi", action="store_true", help="skip the multi-stream section")
+    ap.add_argument("--multi-batches", type=int, default=6, help="batches per stream in the multi-stream section")
     return ap.parse_args()
 
 
@@ -195,18 +201,41 @@ def measured_peak():
 # ---------------------------------------------------------------------------------------
 # scout arm
 # ---------------------------------------------------------------------------------------
-def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, clocks, verbose=False):
+def load_model(path):
+    """Trained scheduler parameters per problem ({"bfs": 6020 floats, "cc": ...}), or {}."""
+    if not path or not os.path.exists(path):
+        return {}
+    d = np.load(path, allow_pickle=False)
+    return {k: np.asarray(d[k], dtype=np.float32) for k in ("bfs", "cc") if k in d.files}
+
+
+def load_tuned(path):
+    """Autotuned knobs: {problem: {"blocks_per_sm", "chunk_log2"}, "round_cap": int}, or {}."""
+    if not path or not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        d = json.load(f)
+    d.pop("report", None)
+    return d
+
+
+def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, clocks, verbose=False, model=None,
+                tune=None):
     import torch
 
     import scout_b200 as sb
     ctx = sb.Context(device)
     ctx.load_csr(off, adj)
     ctx.upload(problem, init)
+    sched = dict(tune or {})
+    if model is not None:
+        ctx.sched_install(problem, model)
+        sched["policy"] = 1
     mirror = init.copy()
     # each step's edits are read from page-locked host memory (copied there before timing)
     batches = [sb.pinned_copy(b) for b in batches[:warmup + steps]]
     for b in batches[:warmup]:
-        ctx.repair(problem, b)
+        ctx.repair(problem, b, sched=sched)
         ctx.commit(problem, mirror)
     timed = batches[warmup:warmup + steps]
     per = []
@@ -220,7 +249,7 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        st = ctx.repair(problem, b)
+        st = ctx.repair(problem, b, sched=sched)
         changed = ctx.commit(problem, mirror)
         e1.record()
         st["commit_changed"] = changed
@@ -235,7 +264,7 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
         e0, e1 = st.pop("_ev")
         st["ms_step"] = e0.elapsed_time(e1)
         if verbose:
-            keep = ("edits", "ms_step", "ms_h2d", "ms_update", "ms_repair", "rounds", "changed", "launches")
+            keep = ("edits", "ms_step", "ms_h2d", "ms_update", "ms_repair", "rounds", "changed", "launches", "variant")
             d = {k: (round(st[k], 3) if isinstance(st[k], float) else st[k]) for k in keep}
             d["phase_ms"] = [round(x, 3) for x in st["phase_ms"]]
             print(problem, json.dumps(d), file=sys.stderr, flush=True)
@@ -277,9 +306,17 @@ def scout_arm(a, dist):
     problems = [p.strip() for p in a.problems.split(",") if p.strip()]
     device = dist.local
     results = {}
+    plain = {}
+    model = load_model(a.model)
+    tuned = load_tuned(a.tuned)
     clocks = Clocks(device)
     for p in problems:
-        results[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks, a.verbose)
+        # the engine as deployed: the learned scheduler where a model exists (BFS, CC) and the
+        # autotuned knobs, and the plain engine (no scheduler, default knobs) beside it
+        results[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks, a.verbose,
+                                 model=model.get(p), tune=tuned.get(p))
+        if p in model or p in tuned:
+            plain[p] = run_problem(p, off, adj, init[p], batches, a.warmup, a.steps, device, dist, clocks, a.verbose)
     clk = clocks.summary()
     peak, peak_kind = measured_peak()
     per_problem = {}
@@ -296,7 +333,16 @@ def scout_arm(a, dist):
                           "batches": len(per), "edits": edits,
                           "repair_ms": sum(s["ms_repair"] for s in per), "update_ms": sum(s["ms_update"] for s in per),
                           "h2d_ms": sum(s["ms_h2d"] for s in per), "rounds": sum(s["rounds"] for s in per),
-                          "changed": sum(s["commit_changed"] for s in per)}
+                          "changed": sum(s["commit_changed"] for s in per),
+                          "scheduler": "learned" if p in model else "plain", "knobs": tuned.get(p, {}),
+                          "variants": [int(s["variant"]) for s in per]}
+        if p in plain:
+            pp, pe = plain[p]
+            pdev = sum(s["ms_update"] + s["ms_repair"] for s in pp)
+            per_problem[p]["plain"] = {"edge_updates_per_s": edits / (pdev / 1e3),
+                                       "e2e_edge_updates_per_s": edits / (pe / 1e3),
+                                       "repair_ms": sum(s["ms_repair"] for s in pp),
+                                       "p99_batch_ms": float(np.percentile([s["ms_step"] for s in pp], 99))}
         tot_edits += edits
         tot_e2e += e2e_ms
         tot_dev += dev_ms
@@ -348,7 +394,133 @@ def scout_arm(a, dist):
     }
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problems, off, adj, init, batches, a.cpu_seconds)
+    if dist.world == 1 and not a.no_multi:
+        del g, off, adj, batches, init
+        line["multi_stream"] = multi_stream(a, device, model, tuned)
     return line
+
+
+# ---------------------------------------------------------------------------------------
+# multi-stream section: 64 independent streams over the four problems and 8 graphs
+# ---------------------------------------------------------------------------------------
+MULTI_GRAPHS = [(14, 8), (15, 16), (16, 32), (17, 8), (18, 16), (19, 32), (20, 8), (22, 16)]
+MULTI_PROBLEMS = ("bfs", "cc", "coloring", "mis")
+
+
+def multi_workload(nbatches: int, seed: int = 7):
+    """64 streams: stream i serves problem i % 4 on graph (i // 4) % 8 (scales 14-22, edge
+    factors 8-32, seeded); each has `nbatches` preferential 50/50 toggle batches whose sizes
+    are log-uniform in [100, 10^6], capped at a quarter of the graph's directed entries. The
+    arrival order interleaves the streams at random (seeded), each stream in its own order."""
+    import scout_b200 as sb
+    rng = np.random.default_rng(seed)
+    graphs = []
+    for gi, (sc, ef) in enumerate(MULTI_GRAPHS):
+        g = sb.gen_rmat(sc, ef, seed=50 + gi)
+        graphs.append(g)
+    streams = []
+    for i in range(64):
+        p = MULTI_PROBLEMS[i % 4]
+        gi = (i // 4) % 8
+        g = graphs[gi]
+        cap = max(100, g.nnz // 4)
+        sizes = [int(min(cap, round(10 ** rng.uniform(2, 6)))) for _ in range(nbatches)]
+        s = g.stream(sb.STREAM_PREFERENTIAL, sum(sizes), 1, insert_ratio=0.5, seed=9000 + i)
+        b = np.cumsum([0] + sizes)
+        streams.append({"problem": p, "graph": gi, "batches": [np.ascontiguousarray(s[b[j]:b[j + 1]])
+                                                                for j in range(nbatches)]})
+    order = np.repeat(np.arange(64), nbatches)
+    rng.shuffle(order)
+    nxt = [0] * 64
+    arrivals = []
+    for i in order.tolist():
+        arrivals.append((i, nxt[i]))
+        nxt[i] += 1
+    return graphs, streams, arrivals
+
+
+def multi_stream(a, device, model, tuned):
+    """Plain (one context per stream, batches one at a time in arrival order), batched (one
+    union store per problem, rounds) and learned+batched (the same with the scheduler model)
+    on the same 64-stream workload. Times: device CUDA events of the library per batch or round
+    (edits already copied), and host wall time of the synchronous calls (copies in, commit out)."""
+    import scout_b200 as sb
+    graphs, streams, arrivals = multi_workload(a.multi_batches)
+    arrays = [g.arrays() for g in graphs]
+    inits = {}
+    for st in streams:
+        key = (st["problem"], st["graph"])
+        if key not in inits:
+            inits[key] = graphs[st["graph"]].init_state(st["problem"], 0)
+    total_edits = sum(len(st["batches"][j]) for st in streams for j in range(len(st["batches"])))
+    out = {"workload": "64 streams (16 per problem: bfs, cc, coloring, mis) over 8 R-MAT graphs "
+                       f"{MULTI_GRAPHS} (scale, edge factor); {a.multi_batches} preferential 50/50 batches per "
+                       "stream, sizes log-uniform in [100, 1e6] capped at nnz/4; seeded random interleaving",
+           "batches": len(arrivals), "edits": int(total_edits)}
+    arms = {"plain": None, "batched": None}
+    if model:
+        arms["learned_batched"] = model
+    res = {k: {"dev_ms": 0.0, "wall_ms": 0.0, "lat": [], "rounds": 0} for k in arms}
+    for p in MULTI_PROBLEMS:
+        sids = [i for i, st in enumerate(streams) if st["problem"] == p]
+        arr_p = [(i, j) for i, j in arrivals if streams[i]["problem"] == p]
+        # plain: a context per stream
+        ctxs, mirrors = {}, {}
+        for i in sids:
+            off, adj = arrays[streams[i]["graph"]]
+            c = sb.Context(device)
+            c.load_csr(off, adj)
+            c.upload(p, inits[(p, streams[i]["graph"])])
+            ctxs[i] = c
+            mirrors[i] = inits[(p, streams[i]["graph"])].copy()
+        pinned = {(i, j): sb.pinned_copy(streams[i]["batches"][j]) for i, j in arr_p}
+        t0 = time.perf_counter()
+        for i, j in arr_p:
+            t1 = time.perf_counter()
+            st = ctxs[i].repair(p, pinned[(i, j)])
+            ctxs[i].commit(p, mirrors[i])
+            res["plain"]["lat"].append(1e3 * (time.perf_counter() - t1))
+            res["plain"]["dev_ms"] += st["ms_update"] + st["ms_repair"]
+        res["plain"]["wall_ms"] += 1e3 * (time.perf_counter() - t0)
+        res["plain"]["rounds"] += len(arr_p)
+        for c in ctxs.values():
+            c.close()
+        # batched (and learned + batched): one union store per problem, rounds of many streams
+        for arm, mdl in arms.items():
+            if arm == "plain":
+                continue
+            me = sb.MultiEngine(p, device)
+            local = {}
+            for i in sids:
+                off, adj = arrays[streams[i]["graph"]]
+                local[i] = me.add_stream(off, adj, inits[(p, streams[i]["graph"])], 0)
+            me.seal()
+            sched = dict(tuned.get(p, {}))
+            if mdl is not None and p in mdl:
+                me.context.sched_install(p, mdl[p])
+                sched["policy"] = 1
+            mir = [inits[(p, streams[i]["graph"])].copy() for i in sids]
+            rounds = sb.form_rounds([(local[i], pinned[(i, j)]) for i, j in arr_p], int(tuned.get("round_cap", 1 << 21)))
+            t0 = time.perf_counter()
+            for rd in rounds:
+                t1 = time.perf_counter()
+                st = me.round(rd, sched=sched)
+                me.commit(mir)
+                dt = 1e3 * (time.perf_counter() - t1)
+                res[arm]["lat"] += [dt] * len(rd)
+                res[arm]["dev_ms"] += st["ms_update"] + st["ms_repair"]
+            res[arm]["wall_ms"] += 1e3 * (time.perf_counter() - t0)
+            res[arm]["rounds"] += len(rounds)
+            me.close()
+    for arm, r in res.items():
+        out[arm] = {"edge_updates_per_s": total_edits / (r["dev_ms"] / 1e3),
+                    "e2e_edge_updates_per_s": total_edits / (r["wall_ms"] / 1e3),
+                    "p50_batch_ms": float(np.percentile(r["lat"], 50)),
+                    "p99_batch_ms": float(np.percentile(r["lat"], 99)), "launch_rounds": r["rounds"]}
+    base = out["plain"]["e2e_edge_updates_per_s"]
+    for arm in arms:
+        out[arm]["e2e_vs_plain"] = out[arm]["e2e_edge_updates_per_s"] / base
+    return out
 
 
 # ---------------------------------------------------------------------------------------

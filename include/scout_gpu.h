@@ -62,11 +62,15 @@ typedef struct scout_sched {
     int32_t policy;           /* scout_policy                                       */
     int32_t mode;             /* scout_mode: incremental repair vs full recompute    */
     int32_t frontier;         /* scout_frontier                                     */
-    int32_t lanes_per_vertex; /* 0 auto; else 1, 2, 4, 8, 32                         */
+    int32_t lanes_per_vertex; /* ignored: every kernel scans rows a warp at a time and
+                                 splits long rows into chunk_log2-sized items instead    */
     int64_t search_bound;     /* CC local-search bound (vertices); 0 = reference rule */
     int64_t search_limit;     /* CC: a class with more deletions left to search than this is
                                  recomputed instead (0 = 32; < 0 = always search)        */
-    int64_t reserved[3];
+    int32_t blocks_per_sm;    /* persistent repair kernels: resident blocks per SM (1..4;
+                                 0 = as many as fit, at most 4)                          */
+    int32_t chunk_log2;       /* BFS queue item = 2^chunk_log2 row entries (8..13; 0 = 10) */
+    int64_t reserved[2];
 } scout_sched;
 
 /* Per-batch statistics (the fields of the reference's Stats structs, scout_bfs.cu:417-424,

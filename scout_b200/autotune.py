@@ -1,0 +1,120 @@
+"""Autotuner of the engine's launch knobs.
+
+Knobs (all exact: they change speed, never results):
+  blocks_per_sm   resident blocks per SM of the persistent repair kernels (1, 2, 4): more
+                  blocks hide latency, fewer make each grid barrier cheaper
+  chunk_log2      BFS queue item = 2^chunk_log2 row entries (8 .. 13): smaller items spread a
+                  hub's row over more warps, larger ones cost fewer queue entries
+  round_cap       multi-stream engine: most edits per round (2^16 .. 2^22): larger rounds
+                  amortise the per-round fixed cost over more streams, smaller ones bound the
+                  latency a small batch waits behind large ones
+The repair variant (incremental, top-down queue traversal, direction-optimizing bitmap
+traversal) is chosen per batch by the scheduler, not here.
+
+Each configuration replays the same sample batches from the same starting state on a fresh
+context and is scored by the library's device time (CUDA events on its stream) over the
+sample, after one warm-up batch.
+
+    python -m scout_b200.autotune --out scout_b200/tuned.json
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import time
+
+import numpy as np
+
+from . import engine as E
+from ._lib import STREAM_PREFERENTIAL
+
+BLOCKS = (1, 2, 4)
+CHUNKS = (8, 10, 12)
+CAPS = (1 << 16, 1 << 18, 1 << 20, 1 << 22)
+
+
+def _device_ms(st: dict) -> float:
+    return st["ms_update"] + st["ms_repair"]
+
+
+def tune_single(problem, off, adj, init, batches, device: int = 0, blocks=BLOCKS, chunks=CHUNKS, model=None) -> dict:
+    """Sweeps blocks_per_sm x chunk_log2 (chunk only matters for BFS) on one stream."""
+    chunks = chunks if problem == "bfs" else (10,)
+    table = []
+    for bps, ch in itertools.product(blocks, chunks):
+        sched = {"blocks_per_sm": bps, "chunk_log2": ch}
+        if model is not None:
+            sched["policy"] = 1
+        with E.Context(device) as ctx:
+            ctx.load_csr(off, adj)
+            ctx.upload(problem, init)
+            if model is not None:
+                ctx.sched_install(problem, model)
+            ctx.repair(problem, batches[0], sched=sched)
+            ms = sum(_device_ms(ctx.repair(problem, b, sched=sched)) for b in batches[1:])
+        table.append({"blocks_per_sm": bps, "chunk_log2": ch, "device_ms": ms})
+    best = min(table, key=lambda r: r["device_ms"])
+    return {"problem": problem, "best": {"blocks_per_sm": best["blocks_per_sm"], "chunk_log2": best["chunk_log2"]},
+            "table": table}
+
+
+def tune_rounds(problem, streams, arrivals, device: int = 0, caps=CAPS, sched=None) -> dict:
+    """Sweeps the multi-stream round cap. streams: [(off, adj, init)], arrivals:
+    [(stream index, edges)] in arrival order. Score: device time + host wall time of the
+    synchronous round calls (the cap trades the two)."""
+    table = []
+    for cap in caps:
+        with E.MultiEngine(problem, device) as me:
+            for off, adj, init in streams:
+                me.add_stream(off, adj, init, 0)
+            me.seal()
+            rounds = E.form_rounds(arrivals, cap)
+            t0 = time.perf_counter()
+            dev = 0.0
+            for rd in rounds:
+                dev += _device_ms(me.round(rd, sched=sched))
+            wall = 1e3 * (time.perf_counter() - t0)
+        table.append({"round_cap": cap, "rounds": len(rounds), "device_ms": dev, "wall_ms": wall})
+    best = min(table, key=lambda r: r["wall_ms"])
+    return {"problem": problem, "best": {"round_cap": best["round_cap"]}, "table": table}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default="")
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args()
+    g = E.gen_rmat(a.scale, 16, seed=2)
+    off, adj = g.arrays()
+    sizes = [10_000, 100_000, 1_000_000, 10_000, 100_000, 1_000_000, 10_000]
+    s = g.stream(STREAM_PREFERENTIAL, sum(sizes), 1, insert_ratio=0.5, seed=77)
+    b = np.cumsum([0] + sizes)
+    batches = [np.ascontiguousarray(s[b[i]:b[i + 1]]) for i in range(len(sizes))]
+    report = {"workload": f"R-MAT scale {a.scale} EF16 seed 2, preferential 50/50 batches {sizes}"}
+    for p in ("bfs", "coloring", "cc", "mis"):
+        r = tune_single(p, off, adj, g.init_state(p, 0), batches, a.device)
+        report[p] = r
+        print(json.dumps(r), flush=True)
+    small = [E.gen_rmat(sc, 16, seed=60 + sc) for sc in (12, 14, 16, 18)]
+    streams = [(h.arrays()[0], h.arrays()[1], h.init_state("bfs", 0)) for h in small for _ in range(4)]
+    rng = np.random.default_rng(5)
+    arrivals = []
+    for j in range(6):
+        for i in rng.permutation(len(streams)):
+            h = small[i // 4]
+            m = int(min(h.nnz // 4, round(10 ** rng.uniform(2, 5))))
+            arrivals.append((int(i), h.stream(STREAM_PREFERENTIAL, m, 1, insert_ratio=0.5, seed=1000 * j + int(i))))
+    report["rounds"] = tune_rounds("bfs", streams, arrivals, a.device)
+    print(json.dumps(report["rounds"]), flush=True)
+    tuned = {p: report[p]["best"] for p in ("bfs", "coloring", "cc", "mis")}
+    tuned["round_cap"] = report["rounds"]["best"]["round_cap"]
+    tuned["report"] = report
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(tuned, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,7 +57,7 @@ int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t s
     int per_sm = 0;
     SCOUT_CU(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
     if (per_sm < 1) return c->fail(SCOUT_E_CUDA, "persistent kernel does not fit on an SM");
-    per_sm = std::min(per_sm, 4);
+    per_sm = std::min(per_sm, c->tune_blocks_per_sm > 0 ? c->tune_blocks_per_sm : 4);
     dim3 grid((unsigned)(per_sm * c->sm_count)), block((unsigned)threads);
     SCOUT_CU(c, cudaLaunchCooperativeKernel(fn, grid, block, args, smem, c->s_main));
     c->nlaunch += 1;
@@ -294,6 +294,17 @@ static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
 }
 
 // Common prologue of a batch: validation, counters, classification + merge of the edits.
+// Tuning knobs of a call: persistent-kernel blocks per SM (1..4, 0 = as many as fit) and the
+// BFS queue item size (2^8 .. 2^13 row entries, 0 = 2^10).
+static int apply_tuning(scout_ctx* c, const scout_sched& sd) {
+    if (sd.blocks_per_sm < 0 || sd.blocks_per_sm > 4) return c->fail(SCOUT_E_INVALID, "blocks_per_sm must be 0..4");
+    if (sd.chunk_log2 != 0 && (sd.chunk_log2 < 8 || sd.chunk_log2 > 13))
+        return c->fail(SCOUT_E_INVALID, "chunk_log2 must be 0 or 8..13");
+    c->tune_blocks_per_sm = sd.blocks_per_sm;
+    c->tune_chunk_log2 = sd.chunk_log2 ? sd.chunk_log2 : 10;
+    return SCOUT_OK;
+}
+
 static int batch_prologue(scout_ctx* c, int problem, const scout_edge* edits, const uint8_t* ops, int64_t m,
                           scout_batch_stats* st) {
     if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
@@ -359,6 +370,7 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     scout_sched sd;
     std::memset(&sd, 0, sizeof(sd));
     if (sched) sd = *sched;
+    SCOUT_RC(apply_tuning(c, sd));
     const int64_t launch0 = c->nlaunch;
     SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
     const int* mode_dev = nullptr;
@@ -392,6 +404,7 @@ int scout_repair_probe(scout_ctx* c, int problem, const scout_edge* edits, const
     scout_sched sd;
     std::memset(&sd, 0, sizeof(sd));
     if (sched) sd = *sched;
+    SCOUT_RC(apply_tuning(c, sd));
     const int64_t launch0 = c->nlaunch;
     SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
     const int* unused = nullptr;

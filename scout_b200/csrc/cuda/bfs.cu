@@ -25,7 +25,6 @@
 namespace scout {
 
 constexpr int BFS_THREADS = 256;
-constexpr int CHUNK = 1024;
 
 struct BfsParams {
     DGraph g;
@@ -49,6 +48,7 @@ struct BfsParams {
     const int* mode_dev;  // when set, the mode is read here (written on the device by the scheduler)
     int32_t* lv_new;      // n: levels of a full traversal before they are diffed into `level`
     long long nnz_pre;    // directed entries before this batch (the batch's delta is in ctr)
+    int chunk, chunk_log2;    // row entries per queue item (a power of two, 256 .. 8192)
     const int32_t* sources;   // when nsrc > 0: every listed vertex is a level-0 root (a union of
     int nsrc;                 // disjoint graphs, one source each); else `source` alone
 };
@@ -56,7 +56,7 @@ struct BfsParams {
 __device__ __forceinline__ int32_t ld_level(const int32_t* p) { return ld_volatile(p); }
 
 // Warp-cooperative push (all 32 lanes call): lanes with `pred` push vertex y into queue qn
-// once per round (tag), split into CHUNK-sized items; first touches of the batch are
+// once per round (tag), split into chunk-sized items; first touches of the batch are
 // appended to the touched list.
 __device__ __forceinline__ void push_vertex(const BfsParams& p, bool pred, int32_t y, int qi, uint32_t tag,
                                             bool chunked, bool touch) {
@@ -72,7 +72,7 @@ __device__ __forceinline__ void push_vertex(const BfsParams& p, bool pred, int32
     if (first) {
         if (chunked) {
             int len = p.g.row[y].len;
-            nit = max(1, (len + CHUNK - 1) / CHUNK);   // an empty row still gets its item
+            nit = max(1, (len + p.chunk - 1) >> p.chunk_log2);   // an empty row still gets its item
         } else {
             nit = 1;
         }
@@ -110,8 +110,8 @@ __device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, 
         int len = 0, lv = -1;
         if (valid) {
             Row r = p.g.row[v];
-            s = r.start + (long long)chunk * CHUNK;
-            len = min(CHUNK, r.len - chunk * CHUNK);
+            s = r.start + ((long long)chunk << p.chunk_log2);
+            len = min(p.chunk, r.len - (chunk << p.chunk_log2));
             if (len < 0) len = 0;
             lv = ld_level(p.level + v);
             if (lv < 0) len = 0;
@@ -154,7 +154,7 @@ constexpr int DO_BETA = 24;    // bottom-up -> top-down once the frontier has < 
 // Warp-cooperative push of newly levelled vertices (each pushed by exactly one lane, so no
 // dedupe tag is needed): chunk items into q[qi], vertex and entry counts into slot qi.
 __device__ __forceinline__ void push_new(const BfsParams& p, bool pred, int32_t y, int len, int qi) {
-    int nit = pred ? max(1, (len + CHUNK - 1) / CHUNK) : 0;
+    int nit = pred ? max(1, (len + p.chunk - 1) >> p.chunk_log2) : 0;
     int incl = warp_incl_scan_i(nit);
     int tot = __shfl_sync(0xffffffffu, incl, WARP - 1);
     if (tot == 0) return;
@@ -191,8 +191,8 @@ __device__ void td_step(const BfsParams& p, int32_t* lv, int cur, int nxt, int d
         int len = 0;
         if (valid) {
             Row r = p.g.row[v];
-            s = r.start + (long long)chunk * CHUNK;
-            len = max(0, min(CHUNK, r.len - chunk * CHUNK));
+            s = r.start + ((long long)chunk << p.chunk_log2);
+            len = max(0, min(p.chunk, r.len - (chunk << p.chunk_log2)));
         }
         int incl = warp_incl_scan_i(len);
         int total = __shfl_sync(0xffffffffu, incl, WARP - 1);
@@ -280,7 +280,7 @@ __device__ bool full_bfs(const BfsParams& p, int mode, long long& bytes, int& ro
             const int32_t s = p.nsrc > 0 ? p.sources[i] : p.source;
             lv[s] = 0;
             const int len = p.g.row[s].len;
-            const int nit = max(1, (len + CHUNK - 1) / CHUNK);
+            const int nit = max(1, (len + p.chunk - 1) >> p.chunk_log2);
             for (int k = 0; k < nit && items + k < p.qcap; k++)
                 p.q[0][items + k] = ((unsigned long long)k << 32) | (uint32_t)s;
             items += nit;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
     }
     {
         // ---- A: invalidation -------------------------------------------------------------
-        // Candidates are queued as CHUNK-sized items of their rows. A single-chunk candidate
+        // Candidates are queued as chunk-sized items of their rows. A single-chunk candidate
         // is settled by one warp (parent check, invalidation, children pushed). A longer one
         // is checked chunk by chunk (any chunk with a valid parent marks found = tag); after
         // a barrier its first item decides, and after another every chunk of an invalidated
@@ -397,14 +397,14 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                 const int32_t c = (int32_t)(item & 0xffffffffu);
                 const int chunk = (int)(item >> 32);
                 const Row r = p.g.row[c];
-                const bool big = r.len > CHUNK;
+                const bool big = r.len > p.chunk;
                 const int lc = ld_level(p.level + c);
                 if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) {
                     if (big && lane_id() == 0) p.found[c] = (int32_t)tag;   // nothing to decide
                     continue;
                 }
-                const long long c0 = (long long)chunk * CHUNK;
-                const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+                const long long c0 = ((long long)chunk << p.chunk_log2);
+                const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
                 const int32_t* rw = p.g.pool + r.start + c0;
                 bool found = false;
                 for (int b0 = 0; b0 < clen && !found; b0 += WARP) {
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     if (i < cnt) {
                         const unsigned long long item = p.q[cur][i];
                         c = (int32_t)(item & 0xffffffffu);
-                        if ((item >> 32) == 0 && p.g.row[c].len > CHUNK && ld_volatile(p.found + c) != (int32_t)tag)
+                        if ((item >> 32) == 0 && p.g.row[c].len > p.chunk && ld_volatile(p.found + c) != (int32_t)tag)
                             nt = atomicExch(&p.st_inval[c], p.epoch) != p.epoch;
                     }
                     int at = warp_append(nt, &p.ctr->list_count[0]);
@@ -465,12 +465,12 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     const unsigned long long item = p.q[cur][i];
                     const int32_t c = (int32_t)(item & 0xffffffffu);
                     const Row r = p.g.row[c];
-                    if (r.len <= CHUNK || ld_volatile(p.found + c) == (int32_t)tag ||
+                    if (r.len <= p.chunk || ld_volatile(p.found + c) == (int32_t)tag ||
                         ld_volatile(p.st_inval + c) != p.epoch)
                         continue;
                     const int lc = ld_level(p.level + c);
-                    const long long c0 = (long long)(item >> 32) * CHUNK;
-                    const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+                    const long long c0 = ((long long)(item >> 32) << p.chunk_log2);
+                    const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
                     const int32_t* rw = p.g.pool + r.start + c0;
                     for (int b0 = 0; b0 < clen; b0 += WARP) {
                         int k = b0 + (int)lane_id();
@@ -519,8 +519,8 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
             const unsigned long long item = p.q[2][i];
             const int32_t c = (int32_t)(item & 0xffffffffu);
             const Row r = p.g.row[c];
-            const long long c0 = (long long)(item >> 32) * CHUNK;
-            const int clen = (int)min((long long)CHUNK, (long long)r.len - c0);
+            const long long c0 = ((long long)(item >> 32) << p.chunk_log2);
+            const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
             const int32_t* rw = p.g.pool + r.start + c0;
             unsigned best = 0xffffffffu;
             for (int b0 = 0; b0 < clen; b0 += WARP) {
@@ -620,6 +620,8 @@ static int bfs_launch(scout_ctx* c, int mode, const int* mode_dev, scout_batch_s
     p.nnz_pre = c->nnz;
     p.sources = c->d_sources;
     p.nsrc = c->nsrc;
+    p.chunk_log2 = c->tune_chunk_log2;
+    p.chunk = 1 << p.chunk_log2;
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_bfs, BFS_THREADS, args, 0);
 }

@@ -155,6 +155,9 @@ struct scout_ctx {
     int64_t last_half = 0;
     int64_t last_aff = 0;
     int32_t coop_blocks = 0;   // resident blocks of the persistent kernels
+    // tuning knobs of the current call (scout_sched.blocks_per_sm / chunk_log2)
+    int tune_blocks_per_sm = 0;   // 0: as many as fit, at most 4
+    int tune_chunk_log2 = 10;     // BFS queue item = 2^chunk_log2 row entries
     int64_t nlaunch = 0;       // kernels launched (running count)
 
     int fail(int code, const std::string& msg) { err = msg; return code; }

@@ -671,8 +671,8 @@ int lists_ensure(scout_ctx* c) {
     SCOUT_RC(graph_ensure_scratch(c));
     if (c->d_list[0]) return SCOUT_OK;
     // Queue items are (chunk << 32 | vertex); a vertex pushed once per round occupies at most
-    // ceil(len / 1024) items, so n + nnz / 1024 + slack bounds a round.
-    c->qcap = c->n + (c->pool_cap / 1024) + 4096;
+    // ceil(len / chunk) items with chunk >= 256 entries, so n + nnz / 256 + slack bounds a round.
+    c->qcap = c->n + (c->pool_cap / 256) + 4096;
     for (int i = 0; i < 3; i++) SCOUT_RC(dev_alloc(c, &c->d_qbuf[i], (size_t)c->qcap * 8, "work queues"));
     for (int i = 0; i < 2; i++) SCOUT_RC(dev_alloc(c, (void**)&c->d_list[i], (size_t)c->n * 4, "vertex lists"));
     SCOUT_RC(dev_alloc(c, (void**)&c->d_commit, (size_t)c->n * 8, "commit pairs"));

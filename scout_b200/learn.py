@@ -152,18 +152,21 @@ def evaluate(params, data: Dataset, problem: str, device: int = 0) -> dict:
             "best": {VARIANT_NAMES[problem][v]: int((ms.argmin(1) == v).sum()) for v in range(nv)}}
 
 
-def default_specs(problem: str, seeds, scales=(16, 18, 20), sizes=(100, 1_000, 10_000, 100_000, 300_000)):
+def default_specs(problem: str, seeds, scales=(16, 18, 20), sizes=(100, 1_000, 10_000, 100_000, 300_000),
+                  graph_seeds=None):
     """Streams spanning the regimes where each variant wins: small batches (incremental),
-    large preferential batches and deletion-heavy low-degree batches (traversals)."""
+    large preferential batches and deletion-heavy low-degree batches (traversals). Stream s
+    runs on graph seed graph_seeds[s % len(graph_seeds)] (default: its own graph, 100 + s)."""
     specs = []
     for s in seeds:
+        gseed = 100 + s if not graph_seeds else graph_seeds[s % len(graph_seeds)]
         for sc in scales:
             cap = 1 << (sc + 2)
             sz = [z for z in sizes if z <= cap]
             seq = [sz[(i * 7 + s) % len(sz)] for i in range(12)]
-            specs.append(StreamSpec(sc, 16, STREAM_PREFERENTIAL, seq, 0.5, graph_seed=100 + s, stream_seed=1000 + s))
-            specs.append(StreamSpec(sc, 16, STREAM_LOWDEG, seq, 0.3, graph_seed=100 + s, stream_seed=2000 + s))
-            specs.append(StreamSpec(sc, 16, STREAM_MIXED, seq, 0.5, graph_seed=100 + s, stream_seed=3000 + s))
+            specs.append(StreamSpec(sc, 16, STREAM_PREFERENTIAL, seq, 0.5, graph_seed=gseed, stream_seed=1000 + s))
+            specs.append(StreamSpec(sc, 16, STREAM_LOWDEG, seq, 0.3, graph_seed=gseed, stream_seed=2000 + s))
+            specs.append(StreamSpec(sc, 16, STREAM_MIXED, seq, 0.5, graph_seed=gseed, stream_seed=3000 + s))
     return specs
 
 
@@ -174,6 +177,7 @@ def main():
     ap.add_argument("--train-seeds", type=int, default=6)
     ap.add_argument("--eval-seeds", type=int, default=2)
     ap.add_argument("--scales", default="16,18,20")
+    ap.add_argument("--sizes", default="100,1000,10000,100000,300000,1000000")
     ap.add_argument("--epochs", type=int, default=400)
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args()
@@ -183,8 +187,11 @@ def main():
     for p in [x.strip() for x in a.problems.split(",") if x.strip()]:
         log = lambda s: print(s, flush=True)  # noqa: E731
         graphs: dict = {}
-        tr = collect(p, default_specs(p, range(a.train_seeds), scales), a.device, graphs=graphs, log=log)
-        ev = collect(p, default_specs(p, range(100, 100 + a.eval_seeds), scales), a.device, graphs=graphs, log=log)
+        sizes = tuple(int(x) for x in a.sizes.split(","))
+        tr = collect(p, default_specs(p, range(a.train_seeds), scales, sizes, graph_seeds=(100, 101)), a.device,
+                     graphs=graphs, log=log)
+        ev = collect(p, default_specs(p, range(100, 100 + a.eval_seeds), scales, sizes, graph_seeds=(200,)),
+                     a.device, graphs=graphs, log=log)
         params, losses = train(tr, a.device, epochs=a.epochs)
         report[p] = {"train_samples": len(tr), "eval_samples": len(ev), "final_loss": float(losses[-1]),
                      "first_loss": float(losses[0]), "eval": evaluate(params, ev, p, a.device),
@@ -192,7 +199,7 @@ def main():
         out[p] = params
         print(json.dumps(report[p]), flush=True)
     if a.out:
-        np.savez(a.out, **out, report=json.dumps(report))
+        np.savez(a.out, **out, report=np.array(json.dumps(report)))
 
 
 if __name__ == "__main__":
