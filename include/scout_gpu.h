@@ -102,6 +102,8 @@ typedef struct scout_batch_stats {
     int64_t variant;      /* repair variant that ran (BFS: 0 incremental, 1 top-down
                              traversal, 2 direction-optimizing traversal; CC: 0
                              incremental, 1 recompute of every class; others 0)     */
+    double  ms_compact;   /* device: pool compaction before the merge (0 when none ran) */
+    int64_t compactions;  /* pool compactions of the context so far                   */
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;
@@ -256,7 +258,14 @@ int scout_multi_commit(scout_multi* m, int32_t* const* mirrors, int64_t* changed
 /* One stream's current solution (n = the stream's vertex count). */
 int scout_multi_download(scout_multi* m, int32_t stream, int32_t* out, int64_t n);
 int scout_multi_streams(scout_multi* m, int32_t* count, int64_t* total_vertices);
+/* scout_reserve of the union for rounds of up to max_round_edits edits (seals first). */
+int scout_multi_reserve(scout_multi* m, int64_t max_round_edits);
 
+/* Allocates, now, every buffer that batches of up to max_edits edits and the uploaded
+ * problems would otherwise grow on first use (workspace, sort and scan partials, work lists,
+ * the compaction target, page-locked commit buffers), so later repairs of that size call no
+ * allocator. No counterpart in the reference (it sizes its buffers per run, scout_mis.cu:802-815). */
+int scout_reserve(scout_ctx* ctx, int64_t max_edits);
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 

@@ -39,7 +39,8 @@ class ScoutBatchStats(C.Structure):
                 ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("ms_update", C.c_double),
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
                 ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
-                ("phase_ms", C.c_double * 4), ("variant", C.c_int64)]
+                ("phase_ms", C.c_double * 4), ("variant", C.c_int64), ("ms_compact", C.c_double),
+                ("compactions", C.c_int64)]
 
     def as_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("reserved", "phase_ms")}
@@ -108,6 +109,8 @@ SIGNATURES = [
     ("scout_multi_commit", C.c_int, [_vp, C.POINTER(_i32p), _i64p]),
     ("scout_multi_download", C.c_int, [_vp, C.c_int32, _i32p, C.c_int64]),
     ("scout_multi_streams", C.c_int, [_vp, _i32p, _i64p]),
+    ("scout_reserve", C.c_int, [_vp, C.c_int64]),
+    ("scout_multi_reserve", C.c_int, [_vp, C.c_int64]),
     ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h
     ("scout_egr_open", C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),

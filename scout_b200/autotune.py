@@ -35,7 +35,7 @@ CAPS = (1 << 16, 1 << 18, 1 << 20, 1 << 22)
 
 
 def _device_ms(st: dict) -> float:
-    return st["ms_update"] + st["ms_repair"]
+    return st["ms_compact"] + st["ms_update"] + st["ms_repair"]
 
 
 def tune_single(problem, off, adj, init, batches, device: int = 0, blocks=BLOCKS, chunks=CHUNKS, model=None) -> dict:
@@ -51,6 +51,7 @@ def tune_single(problem, off, adj, init, batches, device: int = 0, blocks=BLOCKS
             ctx.upload(problem, init)
             if model is not None:
                 ctx.sched_install(problem, model)
+            ctx.reserve_batches(max(len(b) for b in batches))
             ctx.repair(problem, batches[0], sched=sched)
             ms = sum(_device_ms(ctx.repair(problem, b, sched=sched)) for b in batches[1:])
         table.append({"blocks_per_sm": bps, "chunk_log2": ch, "device_ms": ms})
@@ -69,6 +70,7 @@ def tune_rounds(problem, streams, arrivals, device: int = 0, caps=CAPS, sched=No
             for off, adj, init in streams:
                 me.add_stream(off, adj, init, 0)
             me.seal()
+            me.reserve_batches(max(cap, max(len(b) for _, b in arrivals)))
             rounds = E.form_rounds(arrivals, cap)
             t0 = time.perf_counter()
             dev = 0.0

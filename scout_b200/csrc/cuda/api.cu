@@ -78,7 +78,7 @@ static void release(scout_ctx* c) {
     void* hosts[] = {c->h_ctr, c->h_bar, c->h_pin_edits, c->h_pin_commit, c->h_slab[0], c->h_slab[1],
                      c->h_slab_off[0], c->h_slab_off[1], c->h_slab_ids[0], c->h_slab_ids[1]};
     for (void* p : hosts) if (p) cudaFreeHost(p);
-    for (int i = 0; i < 6; i++) if (c->ev_t[i]) cudaEventDestroy(c->ev_t[i]);
+    for (int i = 0; i < 8; i++) if (c->ev_t[i]) cudaEventDestroy(c->ev_t[i]);
     for (int i = 0; i < 2; i++) {
         if (c->ev_copy[i]) cudaEventDestroy(c->ev_copy[i]);
         if (c->s_copy[i]) cudaStreamDestroy(c->s_copy[i]);
@@ -172,7 +172,7 @@ int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
         ok = cudaStreamCreateWithFlags(&c->s_copy[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->ev_copy[i], cudaEventDisableTiming) == cudaSuccess;
     }
-    for (int i = 0; i < 6 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
+    for (int i = 0; i < 8 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
     ok = ok && cudaMallocHost((void**)&c->h_ctr, sizeof(DevCounters)) == cudaSuccess &&
          cudaMallocHost((void**)&c->h_bar, sizeof(GridBar)) == cudaSuccess;
     if (!ok) { cudaError_t le = cudaGetLastError(); release(c); return cuda_fail(nullptr, le, "context streams"); }
@@ -283,8 +283,10 @@ static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
     st->hbm_bytes = h.hbm_bytes;
     st->update_bytes = h.update_bytes;
     st->d2h_bytes += sizeof(DevCounters);
-    st->ms_h2d = ev_ms(c->ev_t[0], c->ev_t[3]);
+    st->ms_compact = ev_ms(c->ev_t[6], c->ev_t[7]);
+    st->ms_h2d = ev_ms(c->ev_t[7], c->ev_t[3]);
     st->ms_update = ev_ms(c->ev_t[3], c->ev_t[1]);
+    st->compactions = c->compactions;
     st->launches = c->nlaunch - launch0;
     for (int i = 0; i < 4; i++) {
         unsigned long long a = h.phase_ns[i], b = h.phase_ns[i + 1];
@@ -535,6 +537,19 @@ int scout_recompute_cc(scout_ctx* c, scout_batch_stats* st) {
     st->changed = c->h_ctr->changed;
     c->last_changed = c->h_ctr->changed;
     st->ms_repair = ev_ms(c->ev_t[1], c->ev_t[2]);
+    return SCOUT_OK;
+}
+
+int scout_reserve(scout_ctx* c, int64_t max_edits) {
+    if (!c || max_edits < 0) return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
+    if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
+    cudaSetDevice(c->device);
+    SCOUT_RC(graph_reserve_batch(c, max_edits));
+    if (c->level && !c->bfs_lv) SCOUT_RC(dev_alloc(c, (void**)&c->bfs_lv, (size_t)c->n * 4, "BFS traversal levels"));
+    if (c->label) SCOUT_RC(cc_ensure(c));
+    if (c->color) SCOUT_RC(coloring_ensure(c));
+    SCOUT_RC(pin_grow(c, &c->h_pin_commit, &c->cap_pin_commit, c->n * 8));
+    SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
     return SCOUT_OK;
 }
 

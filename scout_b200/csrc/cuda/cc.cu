@@ -598,7 +598,7 @@ __global__ void k_cc_init(int32_t* __restrict__ uf, int32_t* __restrict__ cnt, i
     }
 }
 
-static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int* mode_dev) {
+int cc_ensure(scout_ctx* c) {
     SCOUT_RC(lists_ensure(c));
     const int64_t n = c->n;
     if (!c->d_cc) {   // uf, cnt, dirty, remf, newmin, vp, firstw, hcnt
@@ -608,6 +608,12 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int
         k_cc_init<<<blocks_for(n, 256), 256, 0, c->s_main>>>(base, base + n, base + 4 * n, base + 6 * n, n);
         SCOUT_LAUNCH(c, "k_cc_init");
     }
+    return SCOUT_OK;
+}
+
+static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int* mode_dev) {
+    SCOUT_RC(cc_ensure(c));
+    const int64_t n = c->n;
     int32_t* base = c->d_cc;
     CcParams p;
     p.g = dgraph(c);

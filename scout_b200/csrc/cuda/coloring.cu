@@ -204,9 +204,7 @@ __global__ void k_fill_marker(int32_t* __restrict__ m, int64_t n) {
         m[v] = UNMARKED;
 }
 
-int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
-    (void)st;
-    SCOUT_RC(lists_ensure(c));
+int coloring_ensure(scout_ctx* c) {
     if (!c->d_misc || c->cap_misc < c->n) {   // per-vertex proposal markers, UNMARKED at rest
         if (c->d_misc) dev_free(c, c->d_misc, (size_t)c->cap_misc * 4);
         c->d_misc = nullptr;
@@ -216,6 +214,13 @@ int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
         k_fill_marker<<<blocks_for(c->n, 256), 256, 0, c->s_main>>>((int32_t*)c->d_misc, c->n);
         SCOUT_LAUNCH(c, "k_fill_marker");
     }
+    return SCOUT_OK;
+}
+
+int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
+    (void)st;
+    SCOUT_RC(lists_ensure(c));
+    SCOUT_RC(coloring_ensure(c));
     ColParams p;
     p.g = dgraph(c);
     p.color = c->color;

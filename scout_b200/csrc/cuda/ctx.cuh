@@ -55,7 +55,7 @@ struct scout_ctx {
     cudaStream_t s_main = nullptr;
     cudaStream_t s_copy[2] = {nullptr, nullptr};
     cudaEvent_t ev_copy[2] = {nullptr, nullptr};
-    cudaEvent_t ev_t[6] = {nullptr};
+    cudaEvent_t ev_t[8] = {nullptr};
     uint64_t budget = 0;
     uint64_t held = 0;
     std::string err;
@@ -213,6 +213,12 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
               unsigned long long** sorted_out);
 // scan.cu: exclusive scan of int64 values in place; *total receives the sum (device ptr or null)
 int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total);
+int sort_reserve(scout_ctx* c, int64_t nkeys);
+// graph.cu: every buffer a batch of up to m edits can grow, allocated now
+int graph_reserve_batch(scout_ctx* c, int64_t m);
+// problem scratch allocated on first use, or ahead of time by scout_reserve
+int cc_ensure(scout_ctx* c);
+int coloring_ensure(scout_ctx* c);
 // graph.cu
 int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m, scout_batch_stats* st);
 int graph_ensure_scratch(scout_ctx* c);

@@ -667,6 +667,22 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     return SCOUT_OK;
 }
 
+int graph_reserve_batch(scout_ctx* c, int64_t m) {
+    SCOUT_RC(lists_ensure(c));
+    SCOUT_RC(ws_ensure(c, m));
+    const int64_t Amax = std::min<int64_t>(2 * m, c->n);
+    SCOUT_RC(dev_grow(c, &c->d_slices, &c->cap_slices, c->pool_cap / SLICE + Amax + 1024, "merge slices"));
+    SCOUT_RC(sort_reserve(c, std::max<int64_t>(2 * c->ws_m, c->n + 1)));
+    if (!c->d_coff) SCOUT_RC(dev_alloc(c, (void**)&c->d_coff, (size_t)(c->n + 1) * sizeof(int64_t), "compaction offsets"));
+    // the compaction target, when the budget leaves room for a second pool
+    if (!c->spare && c->held + (uint64_t)c->pool_cap * 4 <= c->budget / 100 * 85) {
+        SCOUT_RC(dev_alloc(c, (void**)&c->spare, (size_t)c->pool_cap * 4, "element pool"));
+        c->spare_cap = c->pool_cap;
+    }
+    SCOUT_RC(pin_grow(c, &c->h_pin_edits, &c->cap_pin_edits, m * (int64_t)sizeof(scout_edge) + m + 1));
+    return SCOUT_OK;
+}
+
 int lists_ensure(scout_ctx* c) {
     SCOUT_RC(graph_ensure_scratch(c));
     if (c->d_list[0]) return SCOUT_OK;
@@ -816,7 +832,9 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     c->key_bits = B;
     // Free space must hold a rewrite of every live entry plus two entries per edit.
     int64_t need = c->nnz + 2 * m + 1024;
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[6], c->s_main));
     if (c->pool_cap - c->tail < need) SCOUT_RC(graph_compact(c, need, true));
+    SCOUT_CU(c, cudaEventRecord(c->ev_t[7], c->s_main));
     SCOUT_RC(ws_ensure(c, m));
     SCOUT_RC(graph_ensure_scratch(c));
     if (st) st->h2d_bytes += m * (int64_t)sizeof(scout_edge) + (ops ? m : 0);

@@ -260,6 +260,22 @@ int scout_multi_download(scout_multi* m, int32_t stream, int32_t* out, int64_t n
     return SCOUT_OK;
 }
 
+int scout_multi_reserve(scout_multi* m, int64_t max_round_edits) {
+    if (!m) return SCOUT_E_INVALID;
+    SCOUT_RC(multi_seal(m));
+    if (max_round_edits > m->pin_cap) {
+        if (m->pin) cudaFreeHost(m->pin);
+        if (m->pin_ops) cudaFreeHost(m->pin_ops);
+        m->pin = nullptr;
+        m->pin_ops = nullptr;
+        m->pin_cap = 0;
+        SCOUT_CU(m->ctx, cudaHostAlloc((void**)&m->pin, (size_t)max_round_edits * sizeof(scout_edge), cudaHostAllocPortable));
+        SCOUT_CU(m->ctx, cudaHostAlloc((void**)&m->pin_ops, (size_t)max_round_edits, cudaHostAllocPortable));
+        m->pin_cap = max_round_edits;
+    }
+    return scout_reserve(m->ctx, max_round_edits);
+}
+
 int scout_multi_streams(scout_multi* m, int32_t* count, int64_t* total_vertices) {
     if (!m) return SCOUT_E_INVALID;
     if (count) *count = (int32_t)m->streams.size();

@@ -6,6 +6,8 @@
 // ranks equal digits inside a warp with __match_any_sync.
 #include "ctx.cuh"
 
+#include <algorithm>
+
 namespace scout {
 
 constexpr int SORT_THREADS = 256;
@@ -220,6 +222,16 @@ static int scan_any(scout_ctx* c, T* data, int64_t n, int64_t* d_total) {
 }
 
 int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total) { return scan_any(c, data, n, d_total); }
+
+// Sizes the radix histogram and the scan partials for sorts of up to nkeys keys and scans
+// of up to nkeys entries, so later calls allocate nothing.
+int sort_reserve(scout_ctx* c, int64_t nkeys) {
+    const int64_t nblocks = (nkeys + SORT_TILE - 1) / SORT_TILE;
+    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, nblocks * SORT_RADIX, "sort histogram"));
+    const int64_t scan_n = std::max<int64_t>(nblocks * SORT_RADIX, nkeys + 1);
+    SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, (scan_n + SCAN_TILE - 1) / SCAN_TILE + 1, "scan partials"));
+    return SCOUT_OK;
+}
 
 int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, int64_t n, int bits,
               unsigned long long** sorted_out) {

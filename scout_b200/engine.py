@@ -256,6 +256,16 @@ class Context:
         self._c(LIB.scout_recompute_cc(self._h, C.byref(st)))
         return st.as_dict()
 
+    def held_bytes(self) -> int:
+        """Device bytes the context holds (every allocation counts against its budget)."""
+        v = C.c_uint64()
+        self._c(LIB.scout_ctx_info(self._h, None, 0, C.byref(v)))
+        return v.value
+
+    def reserve_batches(self, max_edits: int) -> None:
+        """Allocates now every buffer batches of up to max_edits edits would grow later."""
+        self._c(LIB.scout_reserve(self._h, int(max_edits)))
+
     def sync(self, timeout_us: int = 0) -> None:
         self._c(LIB.scout_sync(self._h, int(timeout_us)))
 
@@ -328,6 +338,9 @@ class MultiEngine:
 
     def seal(self) -> None:
         self._c(LIB.scout_multi_seal(self._h))
+
+    def reserve_batches(self, max_round_edits: int) -> None:
+        self._c(LIB.scout_multi_reserve(self._h, int(max_round_edits)))
 
     def round(self, batches, sched: Optional[dict] = None) -> dict:
         """batches: [(stream_id, edges), ...] with distinct stream ids."""
