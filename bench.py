@@ -61,6 +61,8 @@ def parse_args():
                     help="autotuned launch knobs (python -m scout_b200.autotune); defaults without it")
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-stream section")
     ap.add_argument("--multi-batches", type=int, default=6, help="batches per stream in the multi-stream section")
+    ap.add_argument("--no-ooc", action="store_true", help="skip the out-of-core section")
+    ap.add_argument("--ooc-scale", type=int, default=23)
     return ap.parse_args()
 
 
@@ -399,7 +401,71 @@ def scout_arm(a, dist):
     if dist.world == 1 and not a.no_multi:
         del g, off, adj, batches, init
         line["multi_stream"] = multi_stream(a, device, model, tuned)
+    if dist.world == 1 and not a.no_ooc:
+        line["out_of_core"] = out_of_core(a, device, model, tuned)
     return line
+
+
+# ---------------------------------------------------------------------------------------
+# out-of-core section: a graph 4.3x larger than its HBM pool (the 16 GB / 69 GB ratio)
+# ---------------------------------------------------------------------------------------
+def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
+    """BFS and CC streams of deletion-heavy batches (70% deletions of existing edges, 30% of
+    them with a low-degree first endpoint; 30% uniform insertions) on an R-MAT graph of scale
+    a.ooc_scale, edge factor 32, whose HBM element pool holds 23% of the adjacency: hot rows
+    in HBM, the rest in mapped page-locked host memory read in place. Plain and learned
+    scheduling on the tiered store, and the all-in-HBM engine on the same stream for scale."""
+    import scout_b200 as sb
+    g = sb.gen_rmat(a.ooc_scale, 32, seed=29)
+    off, adj = g.arrays()
+    nnz = int(g.nnz)
+    hbm = int(0.23 * nnz)
+    s = g.stream(sb.STREAM_LOWDEG, m, nbatches, insert_ratio=0.3, lowdeg_frac=0.3, seed=2929)
+    batches = [sb.pinned_copy(x) for x in s.reshape(nbatches, m, 2)]
+    out = {"workload": f"R-MAT scale {a.ooc_scale} EF32 seed 29 ({g.n} vertices, {nnz} directed entries, "
+                       f"{4 * nnz / 1e9:.2f} GB adjacency); HBM pool {hbm} entries (23%); {nbatches} batches of "
+                       f"{m} toggles: 70% deletions (30% low-degree first endpoint), 30% uniform insertions",
+           "vertices": int(g.n), "directed_entries": nnz}
+    for p in ("bfs", "cc"):
+        init = g.init_state(p, 0)
+        res = {}
+        arms = [("tiered_plain", True, None), ("in_hbm_plain", False, None)]
+        if p in model:
+            arms.insert(1, ("tiered_learned", True, model[p]))
+        for arm, tier, mdl in arms:
+            with sb.Context(device) as ctx:
+                if tier:
+                    ctx.load_tiered(off, adj, hbm_entries=hbm)
+                else:
+                    ctx.load_csr(off, adj)
+                ctx.upload(p, init)
+                sched = dict(tuned.get(p, {}))
+                if mdl is not None:
+                    ctx.sched_install(p, mdl)
+                    sched["policy"] = 1
+                ctx.reserve_batches(m)
+                mirror = init.copy()
+                dev = wall = 0.0
+                lat, variants = [], []
+                for b in batches:
+                    t0 = time.perf_counter()
+                    st = ctx.repair(p, b, sched=sched)
+                    ctx.commit(p, mirror)
+                    dt = 1e3 * (time.perf_counter() - t0)
+                    wall += dt
+                    lat.append(dt)
+                    dev += st["ms_compact"] + st["ms_update"] + st["ms_repair"]
+                    variants.append(int(st["variant"]))
+                info = ctx.tier_info()
+            edits = nbatches * m
+            res[arm] = {"edge_updates_per_s": edits / (dev / 1e3), "e2e_edge_updates_per_s": edits / (wall / 1e3),
+                        "p99_batch_ms": float(np.percentile(lat, 99)), "variants": variants,
+                        "hbm_used": info["hbm_used"], "host_used": info["host_used"], "evicted": info["evicted"]}
+        base = res["tiered_plain"]["e2e_edge_updates_per_s"]
+        for r in res.values():
+            r["e2e_vs_tiered_plain"] = r["e2e_edge_updates_per_s"] / base
+        out[p] = res
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -412,9 +478,11 @@ MULTI_PROBLEMS = ("bfs", "cc", "coloring", "mis")
 def multi_workload(nbatches: int, seed: int = 7):
     """64 streams: stream i serves problem i % 4 on graph (i // 4) % 8 (scales 14-22, edge
     factors 8-32, seeded); each has `nbatches` preferential 50/50 toggle batches whose sizes
-    are log-uniform in [100, 10^6], capped at a quarter of the graph's directed entries. The
+    are log-uniform in [100, 10^6], capped at a quarter of the graph's directed entries (and
+    scaled down where a stream would delete more edges than its graph has). The
     arrival order interleaves the streams at random (seeded), each stream in its own order."""
     import scout_b200 as sb
+    from scout_b200.learn import fit_sizes
     rng = np.random.default_rng(seed)
     graphs = []
     for gi, (sc, ef) in enumerate(MULTI_GRAPHS):
@@ -426,7 +494,7 @@ def multi_workload(nbatches: int, seed: int = 7):
         gi = (i // 4) % 8
         g = graphs[gi]
         cap = max(100, g.nnz // 4)
-        sizes = [int(min(cap, round(10 ** rng.uniform(2, 6)))) for _ in range(nbatches)]
+        sizes = fit_sizes([int(min(cap, round(10 ** rng.uniform(2, 6)))) for _ in range(nbatches)], g.nnz, 0.5)
         s = g.stream(sb.STREAM_PREFERENTIAL, sum(sizes), 1, insert_ratio=0.5, seed=9000 + i)
         b = np.cumsum([0] + sizes)
         streams.append({"problem": p, "graph": gi, "batches": [np.ascontiguousarray(s[b[j]:b[j + 1]])

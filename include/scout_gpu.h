@@ -138,6 +138,20 @@ int scout_graph_seal(scout_ctx* ctx);
 int scout_graph_load_csr(scout_ctx* ctx, int64_t n, const int64_t* off, const int32_t* adj);
 int scout_graph_info(scout_ctx* ctx, int64_t* n, int64_t* nnz, int64_t* pool_used,
                      int64_t* pool_cap);
+/* Out-of-core load for graphs larger than the device budget (the reference keeps the base
+ * graph in an mmap and fetches affected rows per round, core/FlashGraph.h:68-83,
+ * scout_bfs.cu:199-229): the highest-degree rows, up to half of an HBM pool of hbm_entries
+ * elements (0 = derived from the budget), are copied to HBM; every other row lives in mapped
+ * page-locked host memory and is read in place by the kernels over the host link. Rows a
+ * batch rewrites move to HBM; when the HBM pool cannot take a batch, its shortest rows are
+ * evicted to the host pool. scout_graph_load_csr switches to this layout by itself when the
+ * budget cannot hold the graph. */
+int scout_graph_load_tiered(scout_ctx* ctx, int64_t n, const int64_t* off, const int32_t* adj,
+                            int64_t hbm_entries);
+/* HBM pool capacity and use, host pool capacity and use (0 when not tiered), entries evicted
+ * from HBM so far, and batches whose rewritten rows went to the host pool. */
+int scout_graph_tier_info(scout_ctx* ctx, int64_t* hbm_cap, int64_t* hbm_used, int64_t* host_cap,
+                          int64_t* host_used, int64_t* evicted, int64_t* host_batches);
 /* Current adjacency, rows ascending, written as CSR (off: n+1 entries). Two-call protocol:
  * with cap < nnz returns SCOUT_E_CAPACITY and stores nnz in off[n]. */
 int scout_graph_download(scout_ctx* ctx, int64_t* off, int32_t* adj, int64_t cap);
@@ -252,6 +266,10 @@ int scout_multi_seal(scout_multi* m);
 int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
                       const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched,
                       scout_batch_stats* stats);
+/* scout_repair_probe of a round's union batch (training data of the scheduler for rounds). */
+int scout_multi_probe(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched,
+                      double* variant_ms, float* features, scout_batch_stats* stats);
 /* Changed entries of the last round into per-stream host mirrors (mirrors[k]: n_k entries, or
  * NULL to skip stream k); *changed receives the number of entries that changed. */
 int scout_multi_commit(scout_multi* m, int32_t* const* mirrors, int64_t* changed);

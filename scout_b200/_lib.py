@@ -70,6 +70,8 @@ SIGNATURES = [
     ("scout_graph_load_csr", C.c_int, [_vp, C.c_int64, _i64p, _i32p]),
     ("scout_graph_info", C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p]),
     ("scout_graph_download", C.c_int, [_vp, _i64p, _i32p, C.c_int64]),
+    ("scout_graph_load_tiered", C.c_int, [_vp, C.c_int64, _i64p, _i32p, C.c_int64]),
+    ("scout_graph_tier_info", C.c_int, [_vp, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]),
     ("scout_graph_compact", C.c_int, [_vp]),
     ("scout_classify", C.c_int, [_vp, _edgep, C.c_int64, _u8p]),
     ("scout_state_upload", C.c_int, [_vp, C.c_int, _i32p, C.c_int64]),
@@ -106,6 +108,8 @@ SIGNATURES = [
     ("scout_multi_seal", C.c_int, [_vp]),
     ("scout_multi_round", C.c_int, [_vp, C.c_int32, _i32p, C.POINTER(_edgep), _i64p, C.POINTER(_u8p),
                                     C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_multi_probe", C.c_int, [_vp, C.c_int32, _i32p, C.POINTER(_edgep), _i64p, C.POINTER(_u8p),
+                                    C.POINTER(ScoutSched), _f64p, _f32p, C.POINTER(ScoutBatchStats)]),
     ("scout_multi_commit", C.c_int, [_vp, C.POINTER(_i32p), _i64p]),
     ("scout_multi_download", C.c_int, [_vp, C.c_int32, _i32p, C.c_int64]),
     ("scout_multi_streams", C.c_int, [_vp, _i32p, _i64p]),

@@ -70,6 +70,7 @@ static void release(scout_ctx* c) {
     if (c->s_main) cudaStreamSynchronize(c->s_main);
     for (int i = 0; i < 2; i++) if (c->s_copy[i]) cudaStreamSynchronize(c->s_copy[i]);
     sched_release(c);
+    if (c->host_pool) { cudaFreeHost(c->host_pool); c->host_pool = nullptr; }
     void* devs[] = {c->row, c->pool, c->spare, c->level, c->color, c->label, c->mis, c->stamp_a, c->stamp_b, c->stamp_c, c->stamp_d,
                     c->aux_v, c->aux_w, c->ws, c->d_qbuf[0], c->d_qbuf[1], c->d_qbuf[2], c->d_list[0], c->d_list[1],
                     c->d_commit, c->d_sort_hist, c->d_scan_tmp, c->d_slices, c->d_coff, c->d_misc, c->d_cc, c->bfs_lv, c->d_sources, c->d_ctr, c->d_bar, c->d_flags, c->d_stage_ids[0],
@@ -243,7 +244,8 @@ int scout_set_source(scout_ctx* c, int32_t s) {
 namespace scout {
 
 // Repair variant a plain (non-learned) schedule asks for: BFS 0 incremental, 1 top-down
-// traversal, 2 direction-optimizing traversal; CC 0 incremental, 1 recompute.
+// traversal, 2 direction-optimizing traversal; CC 0 incremental, 1 recompute of every class
+// (2, recompute of the touched classes, is the scheduler's).
 static int plain_variant(int problem, const scout_sched& sd) {
     if (sd.mode != SCOUT_MODE_RECOMPUTE) return 0;
     if (problem == SCOUT_BFS) return sd.frontier == SCOUT_FRONTIER_QUEUE ? BFS_MODE_TOP_DOWN : BFS_MODE_DIRECTION_OPT;
@@ -255,11 +257,7 @@ static int run_repair(scout_ctx* c, int problem, const scout_sched& sd, int vari
                       scout_batch_stats* st) {
     switch (problem) {
     case SCOUT_BFS: return bfs_repair(c, variant, mode_dev, st);
-    case SCOUT_CC: {
-        scout_sched v = sd;
-        v.mode = variant ? SCOUT_MODE_RECOMPUTE : SCOUT_MODE_INCREMENTAL;
-        return cc_repair(c, &v, mode_dev, st);
-    }
+    case SCOUT_CC: return cc_repair(c, &sd, variant, mode_dev, st);
     case SCOUT_COLORING: return coloring_repair(c, st);
     case SCOUT_MIS: return mis_repair(c, st);
     }
@@ -383,7 +381,7 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
     SCOUT_RC(counters_fetch(c));
     const DevCounters& h = *c->h_ctr;
-    c->tail += h.new_elems;
+    (c->dest_host ? c->host_tail : c->tail) += h.new_elems;
     c->nnz += h.nnz_delta;
     c->qtag += (uint32_t)h.rounds + 8;
     fill_stats(c, st, launch0);
@@ -456,7 +454,7 @@ int scout_repair_probe(scout_ctx* c, int problem, const scout_edge* edits, const
     }
     for (int v = nv; v < 3; v++) variant_ms[v] = -1.0;
     const DevCounters& h = *c->h_ctr;
-    c->tail += h.new_elems;
+    (c->dest_host ? c->host_tail : c->tail) += h.new_elems;
     c->nnz += h.nnz_delta;
     fill_stats(c, st, launch0);
     st->variant = 0;

@@ -57,8 +57,9 @@ struct CcParams {
     int32_t* st_side;   // == epoch: vertex is in a split side this batch
     int32_t epoch;
     int bound;
-    int full;           // 1: recompute every class
-    const int* mode_dev;  // when set, full = (*mode_dev != 0), decided on the device by the scheduler
+    int variant;        // 0 incremental, 1 recompute every class, 2 recompute every class a
+                        // deletion that no common neighbour settles touches (search limit 0)
+    const int* mode_dev;  // when set, the variant is read here (decided on the device by the scheduler)
     DevCounters* ctr;
     GridBar* bar;
 };
@@ -255,7 +256,9 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
     const int nh = ld_volatile(&p.ctr->n_half);
     long long bytes = 0;
     __shared__ int s_task;
-    const int full = p.mode_dev ? (*p.mode_dev != 0) : p.full;
+    const int variant = p.mode_dev ? *p.mode_dev : p.variant;
+    const int full = variant == 1;
+    const int limit = variant == 2 ? 0 : p.search_limit;
 
     phase_mark(&p.ctr->phase_ns[0]);
     if (!full) {
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
                         const int before = atomicAdd(p.hcnt + cls, 1);
                         const int at = atomicAdd(&p.ctr->list_count[0], 1);
                         if (at < p.hard_cap) p.hard[at] = (int32_t)(b + l);
-                        const bool over = at >= p.hard_cap || (p.search_limit >= 0 && before >= p.search_limit);
+                        const bool over = at >= p.hard_cap || (limit >= 0 && before >= limit);
                         if (over && atomicExch(p.dirty + cls, p.epoch) != p.epoch)
                             atomicAdd(&p.ctr->recomputes, 1);
                     }
@@ -611,7 +614,7 @@ int cc_ensure(scout_ctx* c) {
     return SCOUT_OK;
 }
 
-static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int* mode_dev) {
+static int cc_launch(scout_ctx* c, const scout_sched* sched, int variant, const int* mode_dev) {
     SCOUT_RC(cc_ensure(c));
     const int64_t n = c->n;
     int32_t* base = c->d_cc;
@@ -646,7 +649,7 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int
     // shared memory caps it here, and a search that gives up only costs a class recompute.
     int64_t bound = sched && sched->search_bound > 0 ? sched->search_bound : 5000;
     p.bound = (int)std::min<int64_t>(bound, CC_MAX_BOUND);
-    p.full = full;
+    p.variant = variant;
     p.mode_dev = mode_dev;
     p.ctr = c->d_ctr;
     p.bar = c->d_bar;
@@ -659,10 +662,9 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int full, const int
     return coop_launch(c, (const void*)k_cc, CC_THREADS, args, CC_SMEM);
 }
 
-int cc_repair(scout_ctx* c, const scout_sched* sched, const int* mode_dev, scout_batch_stats* st) {
+int cc_repair(scout_ctx* c, const scout_sched* sched, int variant, const int* mode_dev, scout_batch_stats* st) {
     (void)st;
-    int full = sched && sched->mode == SCOUT_MODE_RECOMPUTE ? 1 : 0;
-    return cc_launch(c, sched, full, mode_dev);
+    return cc_launch(c, sched, variant, mode_dev);
 }
 
 int cc_recompute(scout_ctx* c, scout_batch_stats* st) {

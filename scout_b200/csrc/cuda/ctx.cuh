@@ -44,6 +44,7 @@ struct DevCounters {
     int sched_del_hit;        // deletion half-edits meeting the problem's structural test
     int sched_del;            // deletion half-edits
     int decision;             // repair variant the kernels run (read on the device)
+    int sort_err;             // 1: a sort look-back wait timed out, 2: a sort position out of range
     int sched_flags;          // 1 features computed, 2 model applied
     float feat[24];
     float pred[4];
@@ -70,6 +71,17 @@ struct scout_ctx {
     int64_t tail = 0;          // first free pool element (host view)
     int32_t* spare = nullptr;  // previous pool, next compaction target
     int64_t spare_cap = 0;
+    // tiered store (device budget smaller than the graph): cold rows live in mapped page-locked
+    // host memory and are read in place by the kernels; a row is HBM-resident iff
+    // 0 <= start < pool_cap, otherwise start is its element offset from `pool` into host_pool
+    bool tiered = false;
+    int32_t* host_pool = nullptr;   // host pointer (also the device pointer: unified addressing)
+    int64_t host_cap = 0;
+    int64_t host_tail = 0;
+    int64_t evictions = 0;          // rows moved from HBM to the host pool by compactions
+    int64_t evicted_entries = 0;
+    bool dest_host = false;         // this batch's rewritten rows go to the host pool tail
+    int64_t host_batches = 0;       // batches whose rows were rewritten into the host pool
     int64_t compactions = 0;
     bool reserved = false;
     bool sealed = false;
@@ -122,7 +134,7 @@ struct scout_ctx {
     int32_t* d_list[2] = {nullptr, nullptr};         // touched / invalid lists, n each
     int32_t* d_commit = nullptr;                     // (id, value) pairs for the commit (2n)
     uint32_t qtag = 1;                               // per-round dedupe tags, never reused
-    unsigned int* d_sort_hist = nullptr; int64_t cap_hist = 0;
+    unsigned int* d_sort_hist = nullptr; int64_t cap_hist = 0;   // one-sweep control + look-back
     int64_t* d_scan_tmp = nullptr;  int64_t cap_scan = 0;
     void* d_misc = nullptr;         int64_t cap_misc = 0;   // colouring proposal markers
     int32_t* d_cc = nullptr;        // component scratch (7 n int32)
@@ -233,8 +245,9 @@ int counters_fetch(scout_ctx* c); // copies the device counters into c->h_ctr (s
 constexpr int BFS_MODE_INCREMENTAL = 0, BFS_MODE_TOP_DOWN = 1, BFS_MODE_DIRECTION_OPT = 2;
 int bfs_repair(scout_ctx* c, int mode, const int* mode_dev, scout_batch_stats* st);
 int bfs_recompute(scout_ctx* c, int32_t source, scout_batch_stats* st);
-// CC repair variants: 0 incremental, 1 recompute of every class; mode_dev as for BFS.
-int cc_repair(scout_ctx* c, const scout_sched* sched, const int* mode_dev, scout_batch_stats* st);
+// CC repair variants: 0 incremental, 1 recompute of every class, 2 recompute of every class
+// with an unsettled deletion; mode_dev as for BFS.
+int cc_repair(scout_ctx* c, const scout_sched* sched, int variant, const int* mode_dev, scout_batch_stats* st);
 int cc_recompute(scout_ctx* c, scout_batch_stats* st);
 int coloring_repair(scout_ctx* c, scout_batch_stats* st);
 int mis_repair(scout_ctx* c, scout_batch_stats* st);

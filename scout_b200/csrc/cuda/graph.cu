@@ -621,6 +621,57 @@ __global__ void k_rows_compacted(Row* __restrict__ row, const int64_t* __restric
     }
 }
 
+// ---- tiered store ---------------------------------------------------------------------------
+__device__ __forceinline__ bool in_hbm(const Row& r, long long cap) { return r.start >= 0 && r.start < cap; }
+__device__ __forceinline__ int len_bin(int len) { return 31 - __clz(len + 1); }
+
+__global__ void k_row_lens_hbm(const Row* __restrict__ row, int64_t n, long long cap, int64_t* __restrict__ out) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const Row r = row[v];
+        out[v] = in_hbm(r, cap) ? r.len : 0;
+    }
+}
+
+// HBM entries by floor(log2(1 + row length)) (32 bins), for the eviction threshold.
+__global__ void k_hbm_hist(const Row* __restrict__ row, int64_t n, long long cap, unsigned long long* __restrict__ hist) {
+    __shared__ unsigned long long sh[32];
+    if (threadIdx.x < 32) sh[threadIdx.x] = 0;
+    __syncthreads();
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const Row r = row[v];
+        if (in_hbm(r, cap) && r.len > 0) atomicAdd(&sh[len_bin(r.len)], (unsigned long long)r.len);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32 && sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+__global__ void k_row_lens_evict(const Row* __restrict__ row, int64_t n, long long cap, int bins,
+                                 int64_t* __restrict__ out) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const Row r = row[v];
+        out[v] = (in_hbm(r, cap) && r.len > 0 && len_bin(r.len) < bins) ? r.len : 0;
+    }
+}
+
+__global__ void k_rows_evicted(Row* __restrict__ row, const int64_t* __restrict__ off, int64_t n, long long cap,
+                               int bins, long long host_base) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const Row r = row[v];
+        if (in_hbm(r, cap) && r.len > 0 && len_bin(r.len) < bins) row[v] = Row{host_base + off[v], r.len, r.len};
+    }
+}
+
+// After the HBM rows were copied to the new pool: HBM rows point at their copies, host rows
+// keep their address (their offset is re-based on the new pool).
+__global__ void k_rows_compacted_tiered(Row* __restrict__ row, const int64_t* __restrict__ off, int32_t n,
+                                        long long cap, long long rebase) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const Row r = row[v];
+        if (in_hbm(r, cap)) row[v] = Row{(long long)off[v], r.len, r.len};
+        else row[v] = Row{r.start + rebase, r.len, r.cap};
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
@@ -710,6 +761,8 @@ int counters_fetch(scout_ctx* c) {
     if (c->h_ctr->pad)
         return c->fail(SCOUT_E_STATE, "the component labels do not describe the components of the graph "
                                       "(an edge joins two labels); upload a consistent labelling");
+    if (c->h_ctr->sort_err == 1) return c->fail(SCOUT_E_TIMEOUT, "a sort look-back wait timed out");
+    if (c->h_ctr->sort_err) return c->fail(SCOUT_E_STATE, "the sort computed a position out of range");
     if (c->h_bar->err != 0 || c->h_ctr->overflow)
         return c->fail(SCOUT_E_CAPACITY, "a device work list overflowed its capacity");
     return SCOUT_OK;
@@ -729,7 +782,126 @@ int graph_ensure_scratch(scout_ctx* c) {
 // Rewrites the pool so rows are contiguous and leaves at least min_free free elements
 // (the on-device half of compact_flash_graph). With nnz_exact the host's live count is used
 // and nothing waits for the device; otherwise (after staging) the live count is read back.
+static inline long long elem_delta(const int32_t* a, const int32_t* b) {
+    return (long long)(((intptr_t)a - (intptr_t)b) / (intptr_t)sizeof(int32_t));
+}
+
+// Host pool compaction (tiered store), on the host: the host rows are moved down in order of
+// their position (memmove, every destination at or below its source), and the row table is
+// rewritten.
+static int host_compact(scout_ctx* c) {
+    const int64_t n = c->n;
+    SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+    std::vector<Row> rows((size_t)n);
+    SCOUT_CU(c, cudaMemcpy(rows.data(), c->row, (size_t)n * sizeof(Row), cudaMemcpyDeviceToHost));
+    const long long rel = elem_delta(c->host_pool, c->pool);
+    std::vector<int32_t> ids;
+    for (int64_t v = 0; v < n; v++) {
+        const Row& r = rows[v];
+        if (!(r.start >= 0 && r.start < c->pool_cap) && r.len > 0) ids.push_back((int32_t)v);
+    }
+    std::sort(ids.begin(), ids.end(), [&](int32_t a, int32_t b) { return rows[a].start < rows[b].start; });
+    int64_t pos = 0;
+    for (int32_t v : ids) {
+        Row& r = rows[v];
+        const int64_t from = r.start - rel;
+        if (from != pos) std::memmove(c->host_pool + pos, c->host_pool + from, (size_t)r.len * 4);
+        r.start = rel + pos;
+        r.cap = r.len;
+        pos += r.len;
+    }
+    SCOUT_CU(c, cudaMemcpy(c->row, rows.data(), (size_t)n * sizeof(Row), cudaMemcpyHostToDevice));
+    c->host_tail = pos;
+    return SCOUT_OK;
+}
+
+// Tiered compaction: only HBM rows move. When they and min_free do not fit the HBM pool, the
+// shortest ones (whole log2 length classes, shortest first) are evicted to the host pool.
+static int graph_compact_tiered(scout_ctx* c, int64_t min_free) {
+    const int64_t n = c->n;
+    if (!c->d_coff) SCOUT_RC(dev_alloc(c, (void**)&c->d_coff, (size_t)(n + 1) * sizeof(int64_t), "compaction offsets"));
+    int64_t* off = c->d_coff;
+    const int nb = blocks_for(n, 256);
+    auto hbm_live = [&](int64_t* live) -> int {
+        k_row_lens_hbm<<<nb, 256, 0, c->s_main>>>(c->row, n, (long long)c->pool_cap, off);
+        SCOUT_LAUNCH(c, "k_row_lens_hbm");
+        SCOUT_RC(scan_i64(c, off, n, off + n));
+        SCOUT_CU(c, cudaMemcpyAsync(live, off + n, 8, cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        return SCOUT_OK;
+    };
+    int64_t live = 0;
+    SCOUT_RC(hbm_live(&live));
+    if (live + min_free > c->pool_cap) {
+        // 32 histogram slots in the scan partials (free between scans)
+        SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, 64, "scan partials"));
+        unsigned long long* hist = (unsigned long long*)c->d_scan_tmp;
+        SCOUT_CU(c, cudaMemsetAsync(hist, 0, 32 * 8, c->s_main));
+        k_hbm_hist<<<nb, 256, 0, c->s_main>>>(c->row, n, (long long)c->pool_cap, hist);
+        SCOUT_LAUNCH(c, "k_hbm_hist");
+        unsigned long long h[32];
+        SCOUT_CU(c, cudaMemcpyAsync(h, hist, sizeof(h), cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        int bins = 0;
+        int64_t keep = live;
+        while (bins < 32 && keep + min_free > c->pool_cap) keep -= (int64_t)h[bins++];
+        if (keep + min_free > c->pool_cap)
+            return c->fail(SCOUT_E_CAPACITY, "tiered store: the HBM pool cannot hold the rows of one batch");
+        k_row_lens_evict<<<nb, 256, 0, c->s_main>>>(c->row, n, (long long)c->pool_cap, bins, off);
+        SCOUT_LAUNCH(c, "k_row_lens_evict");
+        SCOUT_RC(scan_i64(c, off, n, off + n));
+        int64_t ev = 0;
+        SCOUT_CU(c, cudaMemcpyAsync(&ev, off + n, 8, cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        if (c->host_tail + ev > c->host_cap) {   // the HBM rows and their offsets stay as they are
+            SCOUT_RC(host_compact(c));
+            if (c->host_tail + ev > c->host_cap) return c->fail(SCOUT_E_CAPACITY, "tiered store: the host pool is full");
+        }
+        const int64_t tiles = (n + ev + COPY_UNITS - 1) / COPY_UNITS;
+        k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 32 * c->sm_count)), COPY_THREADS, 0,
+                      c->s_main>>>(c->row, c->pool, c->host_pool + c->host_tail, off, (int32_t)n, (long long)ev);
+        k_rows_evicted<<<nb, 256, 0, c->s_main>>>(c->row, off, n, (long long)c->pool_cap, bins,
+                                                  elem_delta(c->host_pool, c->pool) + c->host_tail);
+        SCOUT_LAUNCH(c, "eviction");
+        c->host_tail += ev;
+        c->evictions++;
+        c->evicted_entries += ev;
+        c->nlaunch += 8;
+        SCOUT_RC(hbm_live(&live));
+    }
+    int64_t cap = c->pool_cap;
+    int32_t* np = nullptr;
+    if (c->spare && c->spare_cap >= cap) {
+        np = c->spare;
+        cap = c->spare_cap;
+        c->spare = nullptr;
+        c->spare_cap = 0;
+    } else {
+        if (c->spare) { dev_free(c, c->spare, (size_t)c->spare_cap * 4); c->spare = nullptr; c->spare_cap = 0; }
+        SCOUT_RC(dev_alloc(c, (void**)&np, (size_t)cap * sizeof(int32_t), "element pool"));
+    }
+    const int64_t tiles = (n + live + COPY_UNITS - 1) / COPY_UNITS;
+    k_copy_rows<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 32 * c->sm_count)), COPY_THREADS, 0,
+                  c->s_main>>>(c->row, c->pool, np, off, (int32_t)n, (long long)live);
+    k_rows_compacted_tiered<<<nb, 256, 0, c->s_main>>>(c->row, off, (int32_t)n, (long long)c->pool_cap,
+                                                       elem_delta(c->pool, np));
+    SCOUT_LAUNCH(c, "tiered compaction");
+    c->nlaunch += 6;
+    if (c->held <= c->budget / 100 * 85) {
+        c->spare = c->pool;
+        c->spare_cap = c->pool_cap;
+    } else {
+        dev_free(c, c->pool, (size_t)c->pool_cap * sizeof(int32_t));
+    }
+    c->compactions++;
+    c->pool = np;
+    c->pool_cap = cap;
+    c->tail = live;
+    return SCOUT_OK;
+}
+
 int graph_compact(scout_ctx* c, int64_t min_free, bool nnz_exact) {
+    if (c->tiered) return graph_compact_tiered(c, min_free);
     const int64_t n = c->n;
     if (!c->d_coff) SCOUT_RC(dev_alloc(c, (void**)&c->d_coff, (size_t)(n + 1) * sizeof(int64_t), "compaction offsets"));
     int64_t* off = c->d_coff;
@@ -830,8 +1002,9 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     const int64_t n = c->n;
     const int B = key_bits_for(n);
     c->key_bits = B;
-    // Free space must hold a rewrite of every live entry plus two entries per edit.
-    int64_t need = c->nnz + 2 * m + 1024;
+    // Free space must hold a rewrite of every live entry plus two entries per edit (tiered
+    // store: the batch's exact growth is checked after the row allocation instead).
+    int64_t need = c->tiered ? 2 * m + 1024 : c->nnz + 2 * m + 1024;
     SCOUT_CU(c, cudaEventRecord(c->ev_t[6], c->s_main));
     if (c->pool_cap - c->tail < need) SCOUT_RC(graph_compact(c, need, true));
     SCOUT_CU(c, cudaEventRecord(c->ev_t[7], c->s_main));
@@ -860,18 +1033,49 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     k_seg_tails<<<nbh, 256, 0, c->s_main>>>(sorted, B, c->d_ctr, c->d_aff_seg, c->aux_w);
     SCOUT_LAUNCH(c, "segments");
     c->nlaunch += 2;
-    SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
     // merge slices: the long rows' ceil(len / SLICE) sum to at most nnz / SLICE + Amax
     SCOUT_RC(dev_grow(c, &c->d_slices, &c->cap_slices, c->nnz / SLICE + Amax + 1024, "merge slices"));
-    SCOUT_CU(c, cudaMemsetAsync(c->d_small_off, 0, (size_t)(Amax + 1) * 8, c->s_main));
-    k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg, c->d_old_row,
-                                                              c->d_aff_len, c->d_aff_small, c->d_small_off, c->d_slices,
-                                                              c->cap_slices);
-    SCOUT_LAUNCH(c, "k_row_alloc");
-    c->nlaunch += 1;
-    // Exclusive scan over Amax + 1 entries (the tail entries are zero): the new row of affected
-    // row a starts at tail + off[a]; the total is this batch's pool growth.
-    SCOUT_RC(scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems));
+    auto row_alloc = [&](bool again) -> int {
+        SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
+        SCOUT_CU(c, cudaMemsetAsync(c->d_small_off, 0, (size_t)(Amax + 1) * 8, c->s_main));
+        if (again) SCOUT_CU(c, cudaMemsetAsync(&c->d_ctr->n_small, 0, 4 * sizeof(int), c->s_main));   // n_small .. n_pad
+        k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg,
+                                                                  c->d_old_row, c->d_aff_len, c->d_aff_small,
+                                                                  c->d_small_off, c->d_slices, c->cap_slices);
+        SCOUT_LAUNCH(c, "k_row_alloc");
+        c->nlaunch += 1;
+        // Exclusive scan over Amax + 1 entries (the tail entries are zero): the new row of
+        // affected row a starts at tail + off[a]; the total is this batch's pool growth.
+        return scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems);
+    };
+    SCOUT_RC(row_alloc(false));
+    c->dest_host = false;
+    long long dest = c->tail;   // element offset from the HBM pool where the new rows start
+    if (c->tiered) {
+        // the exact growth, before anything is written: compact (evicting short rows to the
+        // host pool) when the HBM pool cannot take it; a batch larger than three quarters of
+        // the HBM pool writes its rows to the host pool instead
+        long long grow = 0;
+        SCOUT_CU(c, cudaMemcpyAsync(&grow, &c->d_ctr->new_elems, 8, cudaMemcpyDeviceToHost, c->s_main));
+        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+        if (c->tail + grow + 1024 > c->pool_cap) {
+            if (grow + 1024 <= c->pool_cap / 4 * 3) {
+                SCOUT_RC(graph_compact(c, grow + 1024, true));
+                SCOUT_RC(row_alloc(true));
+                dest = c->tail;
+            } else {
+                if (c->host_tail + grow > c->host_cap) {
+                    SCOUT_RC(host_compact(c));
+                    if (c->host_tail + grow > c->host_cap)
+                        return c->fail(SCOUT_E_CAPACITY, "tiered store: the host pool cannot take this batch's rows");
+                    SCOUT_RC(row_alloc(true));
+                }
+                c->dest_host = true;
+                c->host_batches++;
+                dest = elem_delta(c->host_pool, c->pool) + c->host_tail;
+            }
+        }
+    }
     long long* dpos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
     long long* E = c->d_mdp;   // matched flags, then their exclusive scan (H + 1 entries)
     k_plan_match<<<blocks_for(H, 256), 256, 0, c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->aux_w, c->d_aff_seg,
@@ -881,16 +1085,16 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_RC(scan_i64(c, (int64_t*)E, H + 1, nullptr));
     k_plan_place<<<blocks_for(H, 256), 256, 0, c->s_main>>>(c->pool, c->row, sorted, B, c->d_ctr, c->aux_w,
                                                             c->d_aff_seg, c->d_old_row, c->d_aff_len,
-                                                            (long long)c->tail, dpos, E);
+                                                            dest, dpos, E);
     SCOUT_LAUNCH(c, "k_plan_place");
     SCOUT_RC(scan_i64(c, c->d_small_off, Amax + 1, nullptr));
     const int64_t groups = std::min<int64_t>(c->nnz, Amax * (int64_t)SMALL_LEN) / UNIT + 1;
     k_merge_small<<<blocks_for(groups * WARP, MERGE_THREADS), MERGE_THREADS, 0, c->s_main>>>(
-        c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, (long long)c->tail, c->d_aff_small,
+        c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, dest, c->d_aff_small,
         c->d_small_off);
     k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, 256), 256, 0,
                      c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len,
-                                  (long long)c->tail, E, dpos, c->d_slices, c->cap_slices);
+                                  dest, E, dpos, c->d_slices, c->cap_slices);
     SCOUT_LAUNCH(c, "merge");
     c->nlaunch += 5;
     return SCOUT_OK;
@@ -1044,8 +1248,8 @@ int scout_graph_seal(scout_ctx* c) {
     dev_free(c, list, (size_t)c->n * 4);
     dev_free(c, flags, 16);
     SCOUT_LAUNCH(c, "seal");
-    // Contiguous rows, exact nnz and tail.
-    SCOUT_RC(graph_compact(c, std::max<int64_t>(c->pool_cap - c->tail, 1 << 22)));
+    // Contiguous rows, exact nnz and tail (a tiered load lays its rows out contiguously).
+    if (!c->tiered) SCOUT_RC(graph_compact(c, std::max<int64_t>(c->pool_cap - c->tail, 1 << 22)));
     c->sealed = true;
     return SCOUT_OK;
 }
@@ -1056,6 +1260,10 @@ int scout_graph_load_csr(scout_ctx* c, int64_t n, const int64_t* off, const int3
     if (off[0] != 0 || nnz < 0 || (nnz > 0 && !adj)) return c->fail(SCOUT_E_INVALID, "bad CSR offsets");
     for (int64_t v = 0; v < n; v++)
         if (off[v + 1] < off[v]) return c->fail(SCOUT_E_INVALID, "CSR offsets must be monotone");
+    // A budget that cannot hold the smallest single-tier store (row table, two pools of
+    // 2 nnz + 4M entries, about 160 B of per-vertex state) gets the tiered store.
+    const uint64_t single = (uint64_t)(16 * n + 160 * n) + 2ull * 4ull * (uint64_t)(2 * nnz + (1 << 22));
+    if (c->held + single > c->budget) return scout_graph_load_tiered(c, n, off, adj, 0);
     SCOUT_RC(scout_graph_reserve(c, n, nnz));
     // Elements: contiguous pinned-slab copies on two streams.
     const int64_t SLAB = 1 << 24;
@@ -1078,6 +1286,121 @@ int scout_graph_load_csr(scout_ctx* c, int64_t n, const int64_t* off, const int3
     dev_free(c, d_off, (size_t)(n + 1) * 8);
     c->tail = nnz;
     return scout_graph_seal(c);
+}
+
+// Tiered load: the highest-degree rows (up to half the HBM pool, the rest of it left for rows
+// the batches rewrite) are copied to HBM; every other row goes to a mapped page-locked host
+// pool that the kernels read in place. Rows are sorted here, on the host.
+int scout_graph_load_tiered(scout_ctx* c, int64_t n, const int64_t* off, const int32_t* adj, int64_t hbm_entries) {
+    if (!c || !off || n < 1 || n >= INT32_MAX) return c ? c->fail(SCOUT_E_INVALID, "bad CSR") : SCOUT_E_INVALID;
+    if (c->reserved) return c->fail(SCOUT_E_STATE, "graph already reserved");
+    const int64_t nnz = off[n];
+    if (off[0] != 0 || nnz < 0 || (nnz > 0 && !adj)) return c->fail(SCOUT_E_INVALID, "bad CSR offsets");
+    for (int64_t v = 0; v < n; v++)
+        if (off[v + 1] < off[v] || off[v + 1] - off[v] > INT32_MAX) return c->fail(SCOUT_E_INVALID, "CSR offsets must be monotone");
+    cudaSetDevice(c->device);
+    if (hbm_entries <= 0) {
+        // what the budget leaves after the row table and about 160 B of per-vertex state, for
+        // two HBM pools (the pool and its compaction target)
+        const int64_t fixed = (int64_t)c->held + 16 * n + 160 * n;
+        hbm_entries = std::max<int64_t>(1 << 20, ((int64_t)c->budget - fixed) / 8);
+    }
+    c->n = n;
+    SCOUT_RC(dev_alloc(c, (void**)&c->row, (size_t)n * sizeof(Row), "row table"));
+    c->pool_cap = hbm_entries;
+    SCOUT_RC(dev_alloc(c, (void**)&c->pool, (size_t)c->pool_cap * sizeof(int32_t), "element pool"));
+    c->host_cap = nnz + nnz / 2 + (1 << 20);
+    {
+        void* hp = nullptr;
+        cudaError_t e = cudaHostAlloc(&hp, (size_t)c->host_cap * 4, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) { cudaGetLastError(); return c->fail(SCOUT_E_CAPACITY, std::string("host pool: ") + cudaGetErrorString(e)); }
+        void* dp = nullptr;
+        SCOUT_CU(c, cudaHostGetDevicePointer(&dp, hp, 0));
+        if (dp != hp) return c->fail(SCOUT_E_NODEV, "tiered store needs unified addressing of page-locked memory");
+        c->host_pool = (int32_t*)hp;
+    }
+    c->tiered = true;
+    // placement: hot rows by descending degree while they fit half the HBM pool
+    std::vector<int32_t> order(n);
+    for (int64_t v = 0; v < n; v++) order[v] = (int32_t)v;
+    std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        const int64_t da = off[a + 1] - off[a], db = off[b + 1] - off[b];
+        return da != db ? da > db : a < b;
+    });
+    std::vector<Row> rows(n);
+    std::vector<char> hot(n, 0);
+    int64_t hbm_used = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const int32_t v = order[i];
+        const int64_t d = off[v + 1] - off[v];
+        if (hbm_used + d > hbm_entries / 2) break;
+        rows[v] = Row{hbm_used, (int)d, (int)d};
+        hot[v] = 1;
+        hbm_used += d;
+    }
+    const long long host_rel = elem_delta(c->host_pool, c->pool);
+    int64_t host_used = 0;
+    std::vector<int64_t> hpos(n, -1);
+    for (int64_t v = 0; v < n; v++) {
+        if (hot[v]) continue;
+        const int64_t d = off[v + 1] - off[v];
+        hpos[v] = host_used;
+        rows[v] = Row{host_rel + host_used, (int)d, (int)d};
+        host_used += d;
+    }
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t v = 0; v < n; v++) {
+        if (hpos[v] < 0) continue;
+        int32_t* dst = c->host_pool + hpos[v];
+        const int64_t d = off[v + 1] - off[v];
+        std::memcpy(dst, adj + off[v], (size_t)d * 4);
+        if (!std::is_sorted(dst, dst + d)) std::sort(dst, dst + d);
+    }
+    // hot rows: gathered in HBM order into the pinned slabs, sorted, copied on two streams
+    const int64_t SLAB = 1 << 24;
+    SCOUT_RC(ensure_slabs(c, SLAB, 1024));
+    int s = 0;
+    int64_t i = 0, pos = 0;
+    while (pos < hbm_used) {
+        SCOUT_CU(c, cudaEventSynchronize(c->ev_copy[s]));
+        int32_t* slab = (int32_t*)c->h_slab[s];
+        const int64_t p0 = pos;
+        while (i < n && hot[order[i]]) {
+            const int32_t v = order[i];
+            const int64_t d = off[v + 1] - off[v];
+            if (pos - p0 + d > SLAB) {
+                if (pos == p0) return c->fail(SCOUT_E_CAPACITY, "a row is longer than the staging slab");
+                break;
+            }
+            int32_t* dst = slab + (pos - p0);
+            std::memcpy(dst, adj + off[v], (size_t)d * 4);
+            if (!std::is_sorted(dst, dst + d)) std::sort(dst, dst + d);
+            pos += d;
+            i++;
+        }
+        SCOUT_CU(c, cudaMemcpyAsync(c->pool + p0, slab, (size_t)(pos - p0) * 4, cudaMemcpyHostToDevice, c->s_copy[s]));
+        SCOUT_CU(c, cudaEventRecord(c->ev_copy[s], c->s_copy[s]));
+        s ^= 1;
+    }
+    SCOUT_CU(c, cudaMemcpy(c->row, rows.data(), (size_t)n * sizeof(Row), cudaMemcpyHostToDevice));
+    c->tail = hbm_used;
+    c->host_tail = host_used;
+    c->nnz = nnz;
+    c->reserved = true;
+    c->sealed = false;
+    return scout_graph_seal(c);
+}
+
+int scout_graph_tier_info(scout_ctx* c, int64_t* hbm_cap, int64_t* hbm_used, int64_t* host_cap, int64_t* host_used,
+                          int64_t* evictions, int64_t* host_batches) {
+    if (!c) return SCOUT_E_INVALID;
+    if (host_batches) *host_batches = c->host_batches;
+    if (hbm_cap) *hbm_cap = c->pool_cap;
+    if (hbm_used) *hbm_used = c->tail;
+    if (host_cap) *host_cap = c->tiered ? c->host_cap : 0;
+    if (host_used) *host_used = c->tiered ? c->host_tail : 0;
+    if (evictions) *evictions = c->evicted_entries;
+    return SCOUT_OK;
 }
 
 int scout_graph_info(scout_ctx* c, int64_t* n, int64_t* nnz, int64_t* used, int64_t* cap) {

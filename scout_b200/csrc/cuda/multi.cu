@@ -160,9 +160,15 @@ int scout_multi_seal(scout_multi* m) {
     return multi_seal(m);
 }
 
-int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
-                      const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched,
-                      scout_batch_stats* stats) {
+}  // extern "C"
+
+namespace {
+
+// The union batch of a round in the engine's page-locked buffer: stream-local ids offset
+// into the stream's range; an id outside the stream's graph becomes -1, which the engine
+// skips like any out-of-range edit.
+int assemble(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+             const int64_t* counts, const uint8_t* const* ops, int64_t* total_out, bool* any_ops_out) {
     if (!m || k < 0 || (k > 0 && (!stream_ids || !edits || !counts))) return mfail(m, SCOUT_E_INVALID, "bad round arguments");
     SCOUT_RC(multi_seal(m));
     const int S = (int)m->streams.size();
@@ -190,8 +196,6 @@ int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, cons
         SCOUT_CU(m->ctx, cudaHostAlloc((void**)&m->pin_ops, (size_t)cap, cudaHostAllocPortable));
         m->pin_cap = cap;
     }
-    // the union batch: stream-local ids offset into the stream's range; an id outside the
-    // stream's graph becomes -1, which the engine skips like any out-of-range edit
 #pragma omp parallel for schedule(dynamic, 1) if (total > 65536)
     for (int i = 0; i < k; i++) {
         const scout_multi::Stream& s = m->streams[stream_ids[i]];
@@ -210,7 +214,32 @@ int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, cons
         }
     }
     m->last_round_edits = total;
+    *total_out = total;
+    *any_ops_out = any_ops;
+    return SCOUT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched,
+                      scout_batch_stats* stats) {
+    int64_t total = 0;
+    bool any_ops = false;
+    SCOUT_RC(assemble(m, k, stream_ids, edits, counts, ops, &total, &any_ops));
     return scout_repair(m->ctx, m->problem, m->pin, any_ops ? m->pin_ops : nullptr, total, sched, stats);
+}
+
+int scout_multi_probe(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops, const scout_sched* sched, double* variant_ms,
+                      float* features, scout_batch_stats* stats) {
+    int64_t total = 0;
+    bool any_ops = false;
+    SCOUT_RC(assemble(m, k, stream_ids, edits, counts, ops, &total, &any_ops));
+    return scout_repair_probe(m->ctx, m->problem, m->pin, any_ops ? m->pin_ops : nullptr, total, sched, variant_ms,
+                              features, stats);
 }
 
 int scout_multi_commit(scout_multi* m, int32_t* const* mirrors, int64_t* changed) {

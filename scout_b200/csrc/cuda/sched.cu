@@ -5,12 +5,14 @@
 // (scout_cc.cu:68-69, 469), and a deferred recompute past them (core/local_repair.h:13-26).
 // Here every BFS/CC batch can run one of several exact repair variants (BFS: incremental,
 // top-down traversal, direction-optimizing traversal; CC: incremental, recompute of every
-// class), all with identical results, and the scheduler chooses one on the device, between
+// class, recompute of the classes an unsettled deletion touches), all with identical
+// results, and the scheduler chooses one on the device, between
 // the batch merge and the repair, without a host round trip:
 //   k_sched_feat   per-batch features from the merged batch (affected rows, half-edits and
 //                  the solution as it stood before the repair)
 //   k_sched_infer  the 24-64-64-4 cost model (bf16 parameters, fp32 accumulation) predicts
-//                  log2 of each variant's repair time; the cheapest variant is written to
+//                  log2 of each variant's repair time; the cheapest variant (a variant other
+//                  than the incremental one only for a predicted gain of about 15%) is written to
 //                  ctr->decision, which the persistent repair kernel reads when it starts.
 // Without an installed model the decision stays 0 (incremental): the plain engine.
 //
@@ -35,6 +37,7 @@
 namespace scout {
 
 constexpr int SCHED_BINS = 16;
+constexpr float SCHED_MARGIN = 0.05f;
 
 struct FeatParams {
     const int32_t* aff;
@@ -132,7 +135,10 @@ __global__ void __launch_bounds__(64) k_sched_infer(DevCounters* __restrict__ ct
     if (t == 0) {
         int best = 0;
         if (w) {
-            for (int v = 1; v < nvariants; v++) if (y[v] < y[best]) best = v;
+            // another variant replaces the incremental repair only for a predicted gain of more
+            // than SCHED_MARGIN (log2 microseconds / 4: 0.05 is about 15%)
+            float by = y[0] - SCHED_MARGIN;
+            for (int v = 1; v < nvariants; v++) if (y[v] < by) { best = v; by = y[v]; }
             for (int o = 0; o < OUT; o++) ctr->pred[o] = y[o];
         }
         ctr->decision = best;
@@ -140,7 +146,7 @@ __global__ void __launch_bounds__(64) k_sched_infer(DevCounters* __restrict__ ct
     }
 }
 
-int sched_variants(int problem) { return problem == SCOUT_BFS ? 3 : (problem == SCOUT_CC ? 2 : 1); }
+int sched_variants(int problem) { return problem == SCOUT_BFS || problem == SCOUT_CC ? 3 : 1; }
 
 int sched_decide(scout_ctx* c, int problem, int64_t m, bool use_model, const int** mode_dev) {
     *mode_dev = nullptr;

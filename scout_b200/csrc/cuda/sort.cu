@@ -1,76 +1,182 @@
 // sort.cu -- stable LSD radix sort of 64-bit keys and an exclusive int64 scan.
 //
 // The batch merge groups half-edits by (vertex, op, neighbour) with one sort. Small sorts run
-// in one CTA entirely in shared memory (one launch); larger ones take, per 8-bit digit, tile
-// histograms, a three-kernel scan of the digit-major histogram, and a stable scatter that
-// ranks equal digits inside a warp with __match_any_sync.
+// in one CTA entirely in shared memory (one launch). Larger ones follow the one-sweep scheme
+// (Adinets and Merrill, "Onesweep: a faster least significant digit radix sort for GPUs",
+// 2022): one kernel histograms every 8-bit digit of every pass at once and turns the
+// histograms into global digit offsets; then each pass is ONE kernel whose blocks take tiles in
+// order from an atomic counter, rank their keys stably (each warp ranks its own contiguous 512
+// keys with __match_any_sync), publish their digit counts and obtain the counts of all earlier
+// tiles by a decoupled look-back, and write the tile out through shared memory so that runs of
+// equal digits land contiguously. 1 + passes launches instead of five per pass.
 #include "ctx.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace scout {
 
-constexpr int SORT_THREADS = 256;
-constexpr int SORT_ITEMS = 8;
-constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
 constexpr int SORT_RADIX = 256;
 // 2 * 10240 keys * 8 B + 33 * 256 * 4 B of tables = 197,632 B of dynamic shared memory,
 // under the 220 KB opt-in requested below.
 constexpr int SMALL_SORT_MAX = 10240;
 constexpr int SMALL_SORT_THREADS = 1024;
 
-__global__ void k_sort_hist(const unsigned long long* __restrict__ keys, int64_t n, int shift,
-                            unsigned int* __restrict__ hist, int nblocks) {
-    __shared__ unsigned int h[SORT_RADIX];
-    for (int i = threadIdx.x; i < SORT_RADIX; i += blockDim.x) h[i] = 0;
+// ---- one-sweep radix sort -------------------------------------------------------------------
+constexpr int OS_THREADS = 256;
+constexpr int OS_WARPS = OS_THREADS / WARP;
+constexpr int OS_STEPS = 16;                        // 32-key steps per warp
+constexpr int OS_TILE = OS_THREADS * OS_STEPS;      // 4096 keys per tile
+constexpr int OS_MAX_PASSES = 8;
+// control block in the sort buffer (32-bit words): [pass][256] histograms, then global digit
+// offsets; the done counter; the per-pass tile counters; the look-back entries (64-bit) follow
+constexpr int OS_DONE = OS_MAX_PASSES * SORT_RADIX;
+constexpr int OS_TILECTR = OS_DONE + 1;
+constexpr int OS_CTRL_WORDS = 4096;
+constexpr unsigned long long OS_AGG = 1ull << 32, OS_INC = 2ull << 32;
+constexpr uint64_t OS_WAIT_LIMIT_NS = 2000000000ull;   // 2 s
+
+// Every digit of every pass at once; the last block to finish turns the histograms into
+// exclusive global offsets and resets the tile counters.
+__global__ void __launch_bounds__(OS_THREADS) k_os_hist(const unsigned long long* __restrict__ keys, int64_t n,
+                                                        int passes, unsigned int* __restrict__ ctl) {
+    __shared__ unsigned int h[OS_MAX_PASSES][SORT_RADIX];
+    __shared__ bool last;
+    for (int i = threadIdx.x; i < OS_MAX_PASSES * SORT_RADIX; i += OS_THREADS) (&h[0][0])[i] = 0;
     __syncthreads();
-    int64_t base = (int64_t)blockIdx.x * SORT_TILE;
-    for (int k = 0; k < SORT_ITEMS; k++) {
-        int64_t i = base + (int64_t)k * SORT_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&h[(unsigned)(keys[i] >> shift) & (SORT_RADIX - 1)], 1u);
+    for (int64_t i = blockIdx.x * (int64_t)OS_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * OS_THREADS) {
+        const unsigned long long k = keys[i];
+        for (int p = 0; p < passes; p++) atomicAdd(&h[p][(unsigned)(k >> (8 * p)) & 255u], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) hist[(int64_t)d * nblocks + blockIdx.x] = h[d];
-}
-
-
-// Stable scatter of one tile: chunks of 256 keys, warp ranks via __match_any_sync, cross-warp
-// offsets from a per-warp digit table.
-__global__ void k_sort_scatter(const unsigned long long* __restrict__ keys, unsigned long long* __restrict__ out,
-                               int64_t n, int shift, const unsigned int* __restrict__ hist, int nblocks) {
-    constexpr int NW = SORT_THREADS / WARP;
-    __shared__ unsigned int base[SORT_RADIX];
-    __shared__ unsigned int wh[NW][SORT_RADIX];
-    __shared__ unsigned int tot[SORT_RADIX];
-    const int t = threadIdx.x, w = t / WARP, l = t % WARP;
-    base[t] = hist[(int64_t)t * nblocks + blockIdx.x];
-    int64_t tile = (int64_t)blockIdx.x * SORT_TILE;
-    const unsigned lt = (1u << l) - 1;
-    for (int k = 0; k < SORT_ITEMS; k++) {
-        int64_t i = tile + (int64_t)k * SORT_THREADS + t;
-        bool valid = i < n;
-        unsigned long long key = valid ? keys[i] : 0ull;
-        unsigned d = valid ? (unsigned)(key >> shift) & (SORT_RADIX - 1) : SORT_RADIX;   // invalid: own class
-        for (int j = 0; j < NW; j++) wh[j][t] = 0;
+    for (int p = 0; p < passes; p++)
+        if (h[p][threadIdx.x]) atomicAdd(&ctl[p * SORT_RADIX + threadIdx.x], h[p][threadIdx.x]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&ctl[OS_DONE], 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int p = 0; p < passes; p++) {   // thread d: exclusive prefix of digit d in pass p
+        __shared__ unsigned int col[SORT_RADIX];
+        col[threadIdx.x] = ld_volatile(&ctl[p * SORT_RADIX + threadIdx.x]);
         __syncthreads();
-        unsigned peers = __match_any_sync(0xffffffffu, d);
-        unsigned rank = __popc(peers & lt);
-        if (valid && rank == 0) wh[w][d] = __popc(peers);
-        __syncthreads();
-        {   // thread t owns digit t: exclusive prefix over warps
+        if (threadIdx.x == 0) {
             unsigned run = 0;
-            for (int j = 0; j < NW; j++) {
-                unsigned c = wh[j][t];
-                wh[j][t] = run;
-                run += c;
-            }
-            tot[t] = run;
+            for (int d = 0; d < SORT_RADIX; d++) { const unsigned c = col[d]; col[d] = run; run += c; }
         }
         __syncthreads();
-        if (valid) out[base[d] + wh[w][d] + rank] = key;
+        ctl[p * SORT_RADIX + threadIdx.x] = col[threadIdx.x];
         __syncthreads();
-        base[t] += tot[t];
+    }
+    if (threadIdx.x < OS_MAX_PASSES) ctl[OS_TILECTR + threadIdx.x] = 0;
+    if (threadIdx.x == 0) ctl[OS_DONE] = 0;
+}
+
+// One pass: stable scatter of every tile by the digit at `shift`. stamp tags this pass's
+// look-back entries (entries of earlier passes read as empty).
+__global__ void __launch_bounds__(OS_THREADS) k_os_pass(const unsigned long long* __restrict__ src,
+                                                        unsigned long long* __restrict__ dst, int64_t n, int pass,
+                                                        unsigned int* __restrict__ ctl,
+                                                        unsigned long long* __restrict__ lb, unsigned stamp,
+                                                        int* __restrict__ err) {
+    __shared__ unsigned long long sk[OS_TILE];
+    __shared__ unsigned int wh[OS_WARPS][SORT_RADIX];   // per-warp digit counts, then prefixes
+    __shared__ unsigned int tot[SORT_RADIX], toff[SORT_RADIX];
+    __shared__ long long gbase[SORT_RADIX];
+    __shared__ int s_tile;
+    const int t = threadIdx.x, w = t / WARP, l = (int)lane_id();
+    const int shift = 8 * pass;
+    if (t == 0) s_tile = (int)atomicAdd(&ctl[OS_TILECTR + pass], 1u);
+    for (int j = 0; j < OS_WARPS; j++) wh[j][t] = 0;
+    __syncthreads();
+    const int tile = s_tile;
+    const int64_t t0 = (int64_t)tile * OS_TILE;
+    // each warp ranks its contiguous 512 keys, 32 at a time, in order (stable)
+    unsigned long long key[OS_STEPS];
+    unsigned short lr[OS_STEPS];
+    const unsigned lt = (1u << l) - 1;
+    const int64_t wbase = t0 + (int64_t)w * (OS_STEPS * WARP);
+#pragma unroll
+    for (int s = 0; s < OS_STEPS; s++) {
+        const int64_t i = wbase + s * WARP + l;
+        const bool valid = i < n;
+        key[s] = valid ? src[i] : ~0ull;
+        const unsigned d = valid ? (unsigned)(key[s] >> shift) & 255u : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        unsigned c = 0;
+        if (valid && l == leader) c = wh[w][d];
+        c = __shfl_sync(0xffffffffu, c, leader);
+        lr[s] = (unsigned short)(c + __popc(peers & lt));
+        __syncwarp();
+        if (valid && l == leader) wh[w][d] = c + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {   // thread t owns digit t: prefix over warps (warp order is key order), tile total
+        unsigned run = 0;
+        for (int j = 0; j < OS_WARPS; j++) { const unsigned c = wh[j][t]; wh[j][t] = run; run += c; }
+        tot[t] = run;
+    }
+    // publish this tile's count, then look back over the earlier tiles
+    const unsigned long long tag = (unsigned long long)stamp << 34;
+    unsigned long long* mine = lb + (int64_t)tile * SORT_RADIX + t;
+    if (tile == 0) {
+        atomicExch(mine, tag | OS_INC | tot[t]);
+        gbase[t] = ctl[pass * SORT_RADIX + t];
+    } else {
+        atomicExch(mine, tag | OS_AGG | tot[t]);
+        unsigned long long excl = 0;
+        int j = tile - 1;
+        const uint64_t start = globaltimer_ns();
+        while (j >= 0) {
+            const unsigned long long v = ld_volatile(lb + (int64_t)j * SORT_RADIX + t);
+            if ((v >> 34) == (unsigned long long)stamp && (v & (3ull << 32))) {
+                excl += v & 0xffffffffull;
+                if (v & OS_INC) break;
+                j--;
+                continue;
+            }
+            if (globaltimer_ns() - start > OS_WAIT_LIMIT_NS) { atomicExch(err, 1); break; }
+            __nanosleep(32);
+        }
+        atomicExch(mine, tag | OS_INC | (excl + tot[t]));
+        gbase[t] = (long long)ctl[pass * SORT_RADIX + t] + (long long)excl;
+    }
+    // tile-local digit offsets (exclusive scan of tot)
+    {
+        __shared__ unsigned int ws[OS_WARPS];
+        unsigned x = tot[t], inc = x;
+#pragma unroll
+        for (int o = 1; o < WARP; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (l >= o) inc += y;
+        }
+        if (l == WARP - 1) ws[w] = inc;
         __syncthreads();
+        unsigned wb = 0;
+        for (int j = 0; j < w; j++) wb += ws[j];
+        toff[t] = wb + inc - x;
+    }
+    __syncthreads();
+    // stage the tile in digit order, then write it out: equal digits are contiguous runs
+#pragma unroll
+    for (int s = 0; s < OS_STEPS; s++) {
+        const int64_t i = wbase + s * WARP + l;
+        if (i < n) {
+            const unsigned d = (unsigned)(key[s] >> shift) & 255u;
+            sk[toff[d] + wh[w][d] + lr[s]] = key[s];
+        }
+    }
+    __syncthreads();
+    const int cnt = (int)min((int64_t)OS_TILE, n - t0);
+    for (int j = t; j < cnt; j += OS_THREADS) {
+        const unsigned long long k = sk[j];
+        const unsigned d = (unsigned)(k >> shift) & 255u;
+        const long long pos = gbase[d] + (j - (int)toff[d]);
+        if (pos >= 0 && pos < n) dst[pos] = k;
+        else atomicExch(err, 2);
     }
 }
 
@@ -225,10 +331,21 @@ int scan_i64(scout_ctx* c, int64_t* data, int64_t n, int64_t* d_total) { return 
 
 // Sizes the radix histogram and the scan partials for sorts of up to nkeys keys and scans
 // of up to nkeys entries, so later calls allocate nothing.
+// Look-back stamps are unique across the process (contexts share freed device memory).
+static unsigned next_stamp() {
+    static std::atomic<unsigned> counter{0};
+    unsigned s = 0;
+    while (s == 0) s = (counter.fetch_add(1) + 1) & ((1u << 30) - 1);
+    return s;
+}
+
 int sort_reserve(scout_ctx* c, int64_t nkeys) {
-    const int64_t nblocks = (nkeys + SORT_TILE - 1) / SORT_TILE;
-    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, nblocks * SORT_RADIX, "sort histogram"));
-    const int64_t scan_n = std::max<int64_t>(nblocks * SORT_RADIX, nkeys + 1);
+    const int64_t ntiles = (nkeys + OS_TILE - 1) / OS_TILE;
+    unsigned int* before = c->d_sort_hist;
+    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, OS_CTRL_WORDS + 2 * SORT_RADIX * ntiles, "sort look-back"));
+    if (c->d_sort_hist != before)   // fresh memory: no stale look-back entry may match a stamp
+        SCOUT_CU(c, cudaMemsetAsync(c->d_sort_hist, 0, (size_t)c->cap_hist * 4, c->s_main));
+    const int64_t scan_n = nkeys + 1;
     SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, (scan_n + SCAN_TILE - 1) / SCAN_TILE + 1, "scan partials"));
     return SCOUT_OK;
 }
@@ -250,16 +367,25 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
         c->nlaunch += 1;
         return SCOUT_OK;
     }
-    int nblocks = (int)((n + SORT_TILE - 1) / SORT_TILE);
-    SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, (int64_t)nblocks * SORT_RADIX, "sort histogram"));
+    const int passes = (bits + 7) / 8;
+    if (passes > OS_MAX_PASSES) return c->fail(SCOUT_E_INVALID, "sort keys wider than 64 bits");
+    const int64_t ntiles = (n + OS_TILE - 1) / OS_TILE;
+    SCOUT_RC(sort_reserve(c, n));
+    unsigned int* ctl = c->d_sort_hist;
+    unsigned long long* lb = (unsigned long long*)(ctl + OS_CTRL_WORDS);
+    SCOUT_CU(c, cudaMemsetAsync(ctl, 0, (size_t)(OS_DONE + 1) * 4, c->s_main));
+    const int hb = (int)std::min<int64_t>((n + OS_TILE - 1) / OS_TILE, 4 * (int64_t)c->sm_count);
+    k_os_hist<<<hb, OS_THREADS, 0, c->s_main>>>(keys, n, passes, ctl);
+    SCOUT_LAUNCH(c, "k_os_hist");
+    c->nlaunch += 1;
     unsigned long long* src = keys;
     unsigned long long* dst = alt;
-    for (int shift = 0; shift < bits; shift += 8) {
-        k_sort_hist<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, n, shift, c->d_sort_hist, nblocks);
-        SCOUT_RC(scan_any(c, c->d_sort_hist, (int64_t)nblocks * SORT_RADIX, nullptr));
-        k_sort_scatter<<<nblocks, SORT_THREADS, 0, c->s_main>>>(src, dst, n, shift, c->d_sort_hist, nblocks);
-        SCOUT_LAUNCH(c, "radix pass");
-        c->nlaunch += 2;
+    for (int p = 0; p < passes; p++) {
+        const unsigned stamp = next_stamp();
+        k_os_pass<<<(unsigned)ntiles, OS_THREADS, 0, c->s_main>>>(src, dst, n, p, ctl, lb, stamp,
+                                                                  &c->d_ctr->sort_err);
+        SCOUT_LAUNCH(c, "k_os_pass");
+        c->nlaunch += 1;
         unsigned long long* s = src; src = dst; dst = s;
     }
     *sorted_out = src;

@@ -141,6 +141,20 @@ class Context:
         self._c(LIB.scout_graph_load_csr(self._h, n, _p64(off), _p32(adj)))
         self.n = n
 
+    def load_tiered(self, off, adj, hbm_entries: int = 0) -> None:
+        """Out-of-core load: hot rows in an HBM pool of hbm_entries elements (0: from the
+        budget), the rest in mapped page-locked host memory read in place."""
+        off = _i64(off)
+        adj = _i32(adj)
+        self._c(LIB.scout_graph_load_tiered(self._h, len(off) - 1, _p64(off), _p32(adj), int(hbm_entries)))
+        self.n = len(off) - 1
+
+    def tier_info(self) -> dict:
+        v = [C.c_int64() for _ in range(6)]
+        self._c(LIB.scout_graph_tier_info(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("hbm_cap", "hbm_used", "host_cap", "host_used", "evicted", "host_batches"),
+                        (x.value for x in v)))
+
     def reserve(self, n: int, nnz: int) -> None:
         self._c(LIB.scout_graph_reserve(self._h, int(n), int(nnz)))
         self.n = int(n)
@@ -355,6 +369,23 @@ class MultiEngine:
             setattr(sd, key, v)
         self._c(LIB.scout_multi_round(self._h, k, _p32(ids), ptrs, _p64(counts), None, C.byref(sd), C.byref(st)))
         return st.as_dict()
+
+    def probe(self, batches, sched: Optional[dict] = None):
+        """A round through Context.repair_probe semantics: (stats, variant_ms[3], features[24])."""
+        k = len(batches)
+        ids = np.array([s for s, _ in batches], dtype=np.int32)
+        arrs = [as_edges(b) for _, b in batches]
+        ptrs = (C.POINTER(ScoutEdge) * max(k, 1))(*[_pedge(a) for a in arrs])
+        counts = np.array([len(a) for a in arrs], dtype=np.int64)
+        st = ScoutBatchStats()
+        sd = ScoutSched()
+        for key, v in (sched or {}).items():
+            setattr(sd, key, v)
+        ms = np.zeros(3, dtype=np.float64)
+        feat = np.zeros(24, dtype=np.float32)
+        self._c(LIB.scout_multi_probe(self._h, k, _p32(ids), ptrs, _p64(counts), None, C.byref(sd),
+                                      ms.ctypes.data_as(C.POINTER(C.c_double)), _pf32(feat), C.byref(st)))
+        return st.as_dict(), ms, feat
 
     def commit(self, mirrors) -> int:
         """mirrors[k]: int32 host mirror of stream k (None to skip)."""

@@ -3,8 +3,9 @@
 The plain engine runs every BFS/CC batch with the incremental repair. The learned engine
 lets a cost model, evaluated on the device after the batch merge, pick among the exact
 repair variants of the problem (BFS: 0 incremental, 1 top-down traversal, 2
-direction-optimizing traversal; CC: 0 incremental, 1 recompute of every class). All
-variants give identical solutions, so the choice only moves time.
+direction-optimizing traversal; CC: 0 incremental, 1 recompute of every class, 2 recompute of
+the classes an unsettled deletion touches). All variants give identical solutions, so the
+choice only moves time.
 
     python -m scout_b200.learn --out scout_b200/sched_model.npz   # collect, train, evaluate
 
@@ -29,9 +30,12 @@ import numpy as np
 from . import engine as E
 from ._lib import STREAM_LOWDEG, STREAM_MIXED, STREAM_PREFERENTIAL
 
-VARIANTS = {"bfs": 3, "cc": 2}
+VARIANTS = {"bfs": 3, "cc": 3}
 VARIANT_NAMES = {"bfs": ["incremental", "top-down traversal", "direction-optimizing traversal"],
-                 "cc": ["incremental", "recompute"]}
+                 "cc": ["incremental", "recompute", "recompute touched classes"]}
+# the device scheduler leaves the incremental repair only for a predicted gain above this
+# (target units: log2(1 + microseconds) / 4, so 0.05 is about 15%)
+MARGIN = 0.05
 
 
 def targets(variant_ms, changed):
@@ -118,6 +122,90 @@ def collect(problem: str, specs, device: int = 0, data: Dataset | None = None, g
     return data
 
 
+@dataclass
+class MultiSpec:
+    """A multi-stream workload: streams_per_graph streams on each seeded graph (scale, edge
+    factor), nbatches batches per stream with log-uniform sizes in [100, 10^6] (capped at a
+    quarter of the graph's entries), kinds drawn per stream, seeded random interleaving, and
+    rounds formed with round_cap."""
+    graphs: list
+    streams_per_graph: int
+    nbatches: int
+    seed: int
+    round_cap: int = 1 << 20
+
+
+def fit_sizes(sizes, nnz: int, insert_ratio: float):
+    """Scales a stream's batch sizes down so its deletions fit the graph: the generators draw
+    distinct existing edges, at most nnz / 2 (undirected) per stream."""
+    limit = int(0.95 * nnz / (2.0 * max(1e-9, 1.0 - insert_ratio)))
+    tot = sum(sizes)
+    if tot <= limit:
+        return list(sizes)
+    return [max(1, int(z * limit / tot)) for z in sizes]
+
+
+def multi_arrivals(spec: MultiSpec, graphs):
+    """(stream graph index, batch) arrivals of a MultiSpec over its generated graphs."""
+    rng = np.random.default_rng(spec.seed)
+    per_stream = []
+    for gi, g in enumerate(graphs):
+        for r in range(spec.streams_per_graph):
+            cap = max(100, g.nnz // 4)
+            sizes = [int(min(cap, round(10 ** rng.uniform(2, 6)))) for _ in range(spec.nbatches)]
+            kind = int(rng.integers(0, 3))
+            ins = 0.5 if kind != STREAM_LOWDEG else 0.3
+            sizes = fit_sizes(sizes, g.nnz, ins)
+            s = g.stream(kind, sum(sizes), 1, insert_ratio=ins,
+                         lowdeg_frac=0.3 if kind == STREAM_LOWDEG else 0.0, seed=spec.seed * 1000 + len(per_stream))
+            b = np.cumsum([0] + sizes)
+            per_stream.append((gi, [np.ascontiguousarray(s[b[j]:b[j + 1]]) for j in range(len(sizes))]))
+    order = np.repeat(np.arange(len(per_stream)), spec.nbatches)
+    rng.shuffle(order)
+    nxt = [0] * len(per_stream)
+    arrivals = []
+    for i in order.tolist():
+        arrivals.append((i, per_stream[i][1][nxt[i]]))
+        nxt[i] += 1
+    return per_stream, arrivals
+
+
+def collect_multi(problem: str, specs, device: int = 0, data: Dataset | None = None, log=None) -> Dataset:
+    """Probes every round of every multi-stream workload (the union batch of the round)."""
+    data = data or Dataset()
+    for spec in specs:
+        graphs = [E.gen_rmat(sc, ef, seed=spec.seed * 100 + i) for i, (sc, ef) in enumerate(spec.graphs)]
+        per_stream, arrivals = multi_arrivals(spec, graphs)
+        t0 = time.time()
+        with E.MultiEngine(problem, device) as me:
+            inits = {}
+            for gi, _ in per_stream:
+                if gi not in inits:
+                    inits[gi] = graphs[gi].init_state(problem, 0)
+                off, adj = graphs[gi].arrays()
+                me.add_stream(off, adj, inits[gi], 0)
+            me.seal()
+            rounds = E.form_rounds(arrivals, spec.round_cap)
+            me.reserve_batches(max(spec.round_cap, max(len(b) for _, b in arrivals)))
+            for rd in rounds:
+                st, ms, f = me.probe(rd)
+                data.add(f, ms, st["changed"], ("multi", len(rd), int(sum(len(b) for _, b in rd))))
+        if log:
+            log(f"{problem}: multi-stream {spec.graphs} x{spec.streams_per_graph}: {len(rounds)} rounds in "
+                f"{time.time() - t0:.1f} s")
+    return data
+
+
+def default_multi_specs(seeds, big: bool = True):
+    """Unions like the benchmark's: 8 graphs of scales 12-22 (or 12-20), two streams each."""
+    out = []
+    for s in seeds:
+        gs = [(12, 8), (14, 16), (15, 32), (16, 8), (17, 16), (18, 32), (20, 8)] + ([(22, 16)] if big else [(19, 16)])
+        out.append(MultiSpec(gs, 2, 6, seed=s))
+        out.append(MultiSpec(gs[:5], 3, 6, seed=s + 500, round_cap=1 << 18))
+    return out
+
+
 def train(data: Dataset, device: int = 0, epochs: int = 300, batch: int = 128, lr: float = 2e-3, seed: int = 0):
     """Trains the cost model on the device; returns (fp32 parameters, per-epoch loss)."""
     x, t, m, _ = data.arrays()
@@ -127,11 +215,19 @@ def train(data: Dataset, device: int = 0, epochs: int = 300, batch: int = 128, l
 
 
 def choose(params, x, nvariants: int, device: int = 0, bf16: bool = True) -> np.ndarray:
-    """The variant the engine's device scheduler would pick for each feature row."""
+    """The variant the engine's device scheduler picks for each feature row: the cheapest
+    predicted one among those beating the incremental repair by more than MARGIN."""
     with E.MLP(device) as net:
         net.params = params
         y = net.forward(x, bf16=bf16)
-    return np.argmin(y[:, :nvariants], axis=1)
+    pick = np.zeros(len(y), dtype=np.int64)
+    for i in range(len(y)):
+        best, by = 0, np.float32(y[i, 0]) - np.float32(MARGIN)
+        for v in range(1, nvariants):
+            if y[i, v] < by:
+                best, by = v, y[i, v]
+        pick[i] = best
+    return pick
 
 
 def evaluate(params, data: Dataset, problem: str, device: int = 0) -> dict:
@@ -180,6 +276,8 @@ def main():
     ap.add_argument("--sizes", default="100,1000,10000,100000,300000,1000000")
     ap.add_argument("--epochs", type=int, default=400)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--multi-seeds", type=int, default=3)
+    ap.add_argument("--multi-weight", type=int, default=4, help="copies of each union-round sample in training")
     a = ap.parse_args()
     scales = tuple(int(x) for x in a.scales.split(","))
     out = {}
@@ -192,10 +290,21 @@ def main():
                      graphs=graphs, log=log)
         ev = collect(p, default_specs(p, range(100, 100 + a.eval_seeds), scales, sizes, graph_seeds=(200,)),
                      a.device, graphs=graphs, log=log)
-        params, losses = train(tr, a.device, epochs=a.epochs)
-        report[p] = {"train_samples": len(tr), "eval_samples": len(ev), "final_loss": float(losses[-1]),
-                     "first_loss": float(losses[0]), "eval": evaluate(params, ev, p, a.device),
-                     "train_fit": evaluate(params, tr, p, a.device)}
+        trm = collect_multi(p, default_multi_specs(range(1, 1 + a.multi_seeds)), a.device, log=log)
+        evm = collect_multi(p, default_multi_specs([77], big=True)[:1], a.device, log=log)
+        both = Dataset()
+        for d, w in ((tr, 1), (trm, a.multi_weight)):
+            for _ in range(w):
+                both.x += d.x
+                both.t += d.t
+                both.m += d.m
+                both.ms += d.ms
+                both.tag += d.tag
+        params, losses = train(both, a.device, epochs=a.epochs)
+        report[p] = {"train_samples": len(tr), "train_rounds": len(trm), "eval_samples": len(ev),
+                     "eval_rounds": len(evm), "final_loss": float(losses[-1]), "first_loss": float(losses[0]),
+                     "eval": evaluate(params, ev, p, a.device), "eval_rounds_result": evaluate(params, evm, p, a.device),
+                     "train_fit": evaluate(params, tr, p, a.device), "train_rounds_fit": evaluate(params, trm, p, a.device)}
         out[p] = params
         print(json.dumps(report[p]), flush=True)
     if a.out:

@@ -1,0 +1,43 @@
+"""Out-of-core (tiered) graph store: hot rows in a small HBM pool, the rest in mapped
+page-locked host memory read in place, rewritten rows moved to HBM, short rows evicted back
+to the host pool when the HBM pool fills. After every batch the adjacency and the solution
+must equal an ordinary single-tier context's, bit for bit, for all four problems."""
+import numpy as np
+import pytest
+
+import scout_b200 as sb
+from gpu_util import stream
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("problem", ["bfs", "cc", "coloring", "mis"])
+def test_tiered_equals_single_tier(rmat16, problem):
+    g, (off, adj) = rmat16
+    init = g.init_state(problem, 0)
+    batches = (list(stream(off, adj, sb.STREAM_PREFERENTIAL, 30000, 2, seed=91))
+               + list(stream(off, adj, sb.STREAM_PREFERENTIAL, 200, 8, seed=94))
+               + list(stream(off, adj, sb.STREAM_LOWDEG, 20000, 2, seed=92, insert_ratio=0.3, lowdeg_frac=0.3))
+               + list(stream(off, adj, sb.STREAM_MIXED, 400, 3, seed=93)))
+    nnz = len(adj)
+    with sb.Context(0) as t, sb.Context(0) as ref:
+        t.load_tiered(off, adj, hbm_entries=nnz // 3)
+        ref.load_csr(off, adj)
+        info = t.tier_info()
+        assert info["host_used"] > 0 and info["hbm_used"] <= nnz // 6 + 1
+        for c in (t, ref):
+            c.upload(problem, init)
+        mt, mr = init.copy(), init.copy()
+        for b in batches:
+            t.repair(problem, b)
+            ref.repair(problem, b)
+            t.commit(problem, mt)
+            ref.commit(problem, mr)
+            assert np.array_equal(t.download(problem), ref.download(problem))
+            assert np.array_equal(mt, mr)
+        o1, a1 = t.graph()
+        o2, a2 = ref.graph()
+        assert np.array_equal(o1, o2) and np.array_equal(a1, a2)
+        info = t.tier_info()
+        assert info["evicted"] > 0, "the medium batches should have made the HBM pool evict rows"
+        assert info["host_batches"] > 0, "the large batches should have written their rows to the host pool"
