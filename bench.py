@@ -62,7 +62,9 @@ def parse_args():
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-stream section")
     ap.add_argument("--multi-batches", type=int, default=6, help="batches per stream in the multi-stream section")
     ap.add_argument("--no-ooc", action="store_true", help="skip the out-of-core section")
-    ap.add_argument("--ooc-scale", type=int, default=23)
+    ap.add_argument("--ooc-scale", type=int, default=21)
+    ap.add_argument("--ooc-batches", type=int, default=4)
+    ap.add_argument("--ooc-edits", type=int, default=250_000)
     return ap.parse_args()
 
 
@@ -190,6 +192,20 @@ class Clocks:
                 "sm_mhz_min": min(self.samples), "sm_mhz_max": max(self.samples),
                 "reasons": sorted(k for k, bit in self.REASONS.items() if self.reasons & bit),
                 "samples": len(self.samples), "source": "NVML, 5 ms polling inside the timed loops"}
+
+
+def profiled_traffic(kernel: str, scale: int):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` on this
+    workload, from the committed ncu summary profiles/roofline_traffic.txt (lines:
+    kernel scale bytes_per_launch), or None when it holds no capture of that kernel and scale."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == kernel and f[1] == str(scale):
+            return float(f[2])
+    return None
 
 
 def measured_peak():
@@ -387,7 +403,7 @@ def scout_arm(a, dist):
         "e2e": {"value": edits_all / e2e_s if e2e_s else None, "unit": "edge-updates/s",
                 "h2d_bytes_per_step": int(h2d / max(n_steps, 1)), "d2h_bytes_per_step": int(d2h / max(n_steps, 1))},
         "roofline": {"bound": "hbm", "kernel": f"k_{kp}", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": profiled_traffic(f"k_{kp}", a.scale),
                      "algorithmic_bytes_per_launch": b / max(nl, 1), "ms_per_launch": ms / max(nl, 1),
                      "launches": nl},
         "roofline_merge": {"kernels": "k_classify .. k_merge_slices (batch merge pipeline)",
@@ -402,7 +418,7 @@ def scout_arm(a, dist):
         del g, off, adj, batches, init
         line["multi_stream"] = multi_stream(a, device, model, tuned)
     if dist.world == 1 and not a.no_ooc:
-        line["out_of_core"] = out_of_core(a, device, model, tuned)
+        line["out_of_core"] = out_of_core(a, device, model, tuned, a.ooc_batches, a.ooc_edits)
     return line
 
 
@@ -456,6 +472,10 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
                     lat.append(dt)
                     dev += st["ms_compact"] + st["ms_update"] + st["ms_repair"]
                     variants.append(int(st["variant"]))
+                    if a.verbose:
+                        print(f"out_of_core {p} {arm}: wall {dt:.1f} ms, update {st['ms_update']:.1f}, repair "
+                              f"{st['ms_repair']:.1f}, compact {st['ms_compact']:.1f}, variant {st['variant']}, "
+                              f"tiers {ctx.tier_info()}", file=sys.stderr, flush=True)
                 info = ctx.tier_info()
             edits = nbatches * m
             res[arm] = {"edge_updates_per_s": edits / (dev / 1e3), "e2e_edge_updates_per_s": edits / (wall / 1e3),

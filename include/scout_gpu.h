@@ -284,6 +284,13 @@ int scout_multi_reserve(scout_multi* m, int64_t max_round_edits);
  * the compaction target, page-locked commit buffers), so later repairs of that size call no
  * allocator. No counterpart in the reference (it sizes its buffers per run, scout_mis.cu:802-815). */
 int scout_reserve(scout_ctx* ctx, int64_t max_edits);
+/* Initial solution of a problem computed on the device from the current graph, replacing the
+ * reference's offline seeding tools: greedy MIS in vertex-id order
+ * (tools/compute_initial_mis.py:32-43), greedy smallest-free colouring in vertex-id order
+ * (tools/greedy_color.cpp:37-52), BFS levels from source (tools/bfs_ground_truth.cu:39-151),
+ * min-vertex-id component labels (tools/excc_src/excc_v1.cu:520-531). The state is allocated
+ * if none was uploaded; read it with scout_state_download. */
+int scout_seed(scout_ctx* ctx, int problem, int32_t source, scout_batch_stats* stats);
 /* Waits for all work of the context, at most timeout_us (<= 0: no limit). */
 int scout_sync(scout_ctx* ctx, int64_t timeout_us);
 

@@ -114,6 +114,7 @@ SIGNATURES = [
     ("scout_multi_download", C.c_int, [_vp, C.c_int32, _i32p, C.c_int64]),
     ("scout_multi_streams", C.c_int, [_vp, _i32p, _i64p]),
     ("scout_reserve", C.c_int, [_vp, C.c_int64]),
+    ("scout_seed", C.c_int, [_vp, C.c_int, C.c_int32, C.POINTER(ScoutBatchStats)]),
     ("scout_multi_reserve", C.c_int, [_vp, C.c_int64]),
     ("scout_bfs_levels_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p]),
     # scout_host.h

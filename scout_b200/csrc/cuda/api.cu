@@ -264,6 +264,13 @@ static int run_repair(scout_ctx* c, int problem, const scout_sched& sd, int vari
     return c->fail(SCOUT_E_INVALID, "unknown problem");
 }
 
+// The pool tails after a batch's merge (where its rewritten rows went).
+static void advance_tails(scout_ctx* c, const DevCounters& h) {
+    if (c->batch_dest == 1) c->host_tail += h.new_elems;
+    else c->tail += h.new_elems;
+    if (c->batch_dest == 2) c->host_tail += h.new_elems_host;
+}
+
 // Batch statistics from the counters of the last repair run (already fetched).
 static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
     const DevCounters& h = *c->h_ctr;
@@ -381,7 +388,7 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
     SCOUT_RC(counters_fetch(c));
     const DevCounters& h = *c->h_ctr;
-    (c->dest_host ? c->host_tail : c->tail) += h.new_elems;
+    advance_tails(c, h);
     c->nnz += h.nnz_delta;
     c->qtag += (uint32_t)h.rounds + 8;
     fill_stats(c, st, launch0);
@@ -454,7 +461,7 @@ int scout_repair_probe(scout_ctx* c, int problem, const scout_edge* edits, const
     }
     for (int v = nv; v < 3; v++) variant_ms[v] = -1.0;
     const DevCounters& h = *c->h_ctr;
-    (c->dest_host ? c->host_tail : c->tail) += h.new_elems;
+    advance_tails(c, h);
     c->nnz += h.nnz_delta;
     fill_stats(c, st, launch0);
     st->variant = 0;

@@ -20,7 +20,8 @@ struct DevCounters {
     int n_aff;          // vertices whose row changed
     int n_small, n_large;     // rows planned by a warp / by a block
     int n_slices, n_pad;      // merge slices
-    long long new_elems;      // elements written to the pool this batch
+    long long new_elems;      // elements written to the pool this batch (HBM part when split)
+    long long new_elems_host; // tiered store, split batch: elements written to the host pool
     long long nnz_delta;      // inserted minus deleted entries
     long long update_bytes;   // algorithmic bytes of the row merge
     // repair
@@ -80,7 +81,8 @@ struct scout_ctx {
     int64_t host_tail = 0;
     int64_t evictions = 0;          // rows moved from HBM to the host pool by compactions
     int64_t evicted_entries = 0;
-    bool dest_host = false;         // this batch's rewritten rows go to the host pool tail
+    int batch_dest = 0;             // where this batch's rewritten rows go: 0 HBM tail, 1 host
+                                    // tail, 2 split (rows from HBM to HBM, host rows to host)
     int64_t host_batches = 0;       // batches whose rows were rewritten into the host pool
     int64_t compactions = 0;
     bool reserved = false;
@@ -121,6 +123,7 @@ struct scout_ctx {
     int32_t* d_aff = nullptr;       // affected vertex ids (2m)
     int64_t* d_aff_seg = nullptr;   // [3 * 2m]: segment begin, first deletion, end
     int64_t* d_aff_len = nullptr;   // new length, then exclusive offsets (2m + 1)
+    int64_t* d_aff_len2 = nullptr;  // tiered split batches: lengths / offsets of the host rows (2m + 1)
     int32_t* d_aff_small = nullptr; // affected rows merged by the short-row merge (2m)
     int64_t* d_small_off = nullptr; // short-row lengths, then their exclusive scan (2m + 1)
     scout::Row* d_old_row = nullptr;   // descriptors of the affected rows before the batch (2m)

@@ -661,6 +661,28 @@ __global__ void k_rows_evicted(Row* __restrict__ row, const int64_t* __restrict_
     }
 }
 
+// Split batches: the allocation of an affected row goes to the host lengths when its old
+// version lives in the host pool (lenH keeps the HBM rows' allocations).
+__global__ void k_split_alloc(const Row* __restrict__ old_row, const DevCounters* __restrict__ ctr, long long cap,
+                              int64_t* __restrict__ lenH, int64_t* __restrict__ lenC) {
+    const int A = ctr->n_aff;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < A; a += gridDim.x * blockDim.x) {
+        if (!in_hbm(old_row[a], cap)) {
+            lenC[a] = lenH[a];
+            lenH[a] = 0;
+        }
+    }
+}
+
+// Absolute destinations (element offsets from the HBM pool) of a split batch's rows.
+__global__ void k_abs_off(const Row* __restrict__ old_row, const DevCounters* __restrict__ ctr, long long cap,
+                          int64_t* __restrict__ offH, const int64_t* __restrict__ offC, long long hbm_base,
+                          long long host_base) {
+    const int A = ctr->n_aff;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < A; a += gridDim.x * blockDim.x)
+        offH[a] = in_hbm(old_row[a], cap) ? hbm_base + offH[a] : host_base + offC[a];
+}
+
 // After the HBM rows were copied to the new pool: HBM rows point at their copies, host rows
 // keep their address (their offset is re-based on the new pool).
 __global__ void k_rows_compacted_tiered(Row* __restrict__ row, const int64_t* __restrict__ off, int32_t n,
@@ -691,7 +713,8 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     size_t sz[] = {
         (size_t)M * sizeof(scout_edge), (size_t)M, (size_t)M,
         (size_t)H * 8, (size_t)H * 8, (size_t)(H + 1) * 8,
-        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)(H + 1) * 8, (size_t)H * sizeof(Row)};
+        (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)(H + 1) * 8, (size_t)H * sizeof(Row),
+        (size_t)(H + 1) * 8};
     size_t total = 0;
     for (size_t s : sz) total += align256(s);
     if (c->ws) dev_free(c, c->ws, (size_t)c->ws_bytes);
@@ -714,6 +737,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     c->d_aff_small = (int32_t*)take(sz[9]);
     c->d_small_off = (int64_t*)take(sz[10]);
     c->d_old_row = (Row*)take(sz[11]);
+    c->d_aff_len2 = (int64_t*)take(sz[12]);
     c->d_hkeys = c->d_keys;
     return SCOUT_OK;
 }
@@ -1035,7 +1059,9 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     c->nlaunch += 2;
     // merge slices: the long rows' ceil(len / SLICE) sum to at most nnz / SLICE + Amax
     SCOUT_RC(dev_grow(c, &c->d_slices, &c->cap_slices, c->nnz / SLICE + Amax + 1024, "merge slices"));
-    auto row_alloc = [&](bool again) -> int {
+    // split: tiered store, rows whose old version lives in HBM are rewritten into HBM and host
+    // rows into the host pool (two scans); otherwise one scan for one destination
+    auto row_alloc = [&](bool again, bool split) -> int {
         SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len, 0, (size_t)(Amax + 1) * 8, c->s_main));
         SCOUT_CU(c, cudaMemsetAsync(c->d_small_off, 0, (size_t)(Amax + 1) * 8, c->s_main));
         if (again) SCOUT_CU(c, cudaMemsetAsync(&c->d_ctr->n_small, 0, 4 * sizeof(int), c->s_main));   // n_small .. n_pad
@@ -1044,36 +1070,61 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
                                                                   c->d_small_off, c->d_slices, c->cap_slices);
         SCOUT_LAUNCH(c, "k_row_alloc");
         c->nlaunch += 1;
+        if (split) {
+            SCOUT_CU(c, cudaMemsetAsync(c->d_aff_len2, 0, (size_t)(Amax + 1) * 8, c->s_main));
+            k_split_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->d_old_row, c->d_ctr, (long long)c->pool_cap,
+                                                                        c->d_aff_len, c->d_aff_len2);
+            SCOUT_LAUNCH(c, "k_split_alloc");
+            c->nlaunch += 1;
+            SCOUT_RC(scan_i64(c, c->d_aff_len2, Amax + 1, (int64_t*)&c->d_ctr->new_elems_host));
+        } else if (again) {
+            SCOUT_CU(c, cudaMemsetAsync(&c->d_ctr->new_elems_host, 0, 8, c->s_main));
+        }
         // Exclusive scan over Amax + 1 entries (the tail entries are zero): the new row of
         // affected row a starts at tail + off[a]; the total is this batch's pool growth.
         return scan_i64(c, c->d_aff_len, Amax + 1, (int64_t*)&c->d_ctr->new_elems);
     };
-    SCOUT_RC(row_alloc(false));
-    c->dest_host = false;
+    c->batch_dest = c->tiered ? 2 : 0;
+    SCOUT_RC(row_alloc(false, c->tiered));
     long long dest = c->tail;   // element offset from the HBM pool where the new rows start
     if (c->tiered) {
-        // the exact growth, before anything is written: compact (evicting short rows to the
-        // host pool) when the HBM pool cannot take it; a batch larger than three quarters of
-        // the HBM pool writes its rows to the host pool instead
-        long long grow = 0;
-        SCOUT_CU(c, cudaMemcpyAsync(&grow, &c->d_ctr->new_elems, 8, cudaMemcpyDeviceToHost, c->s_main));
-        SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
-        if (c->tail + grow + 1024 > c->pool_cap) {
-            if (grow + 1024 <= c->pool_cap / 4 * 3) {
-                SCOUT_RC(graph_compact(c, grow + 1024, true));
-                SCOUT_RC(row_alloc(true));
-                dest = c->tail;
+        // the exact growth, before anything is written. HBM part too large: compact (evicting
+        // short rows to the host pool); larger than three quarters of the HBM pool: the whole
+        // batch goes to the host pool. Host pool full: compacted in place on the host.
+        long long grow[2] = {0, 0};   // HBM, host
+        auto read_grow = [&]() -> int {
+            SCOUT_CU(c, cudaMemcpyAsync(grow, &c->d_ctr->new_elems, 16, cudaMemcpyDeviceToHost, c->s_main));
+            SCOUT_CU(c, cudaStreamSynchronize(c->s_main));
+            return SCOUT_OK;
+        };
+        SCOUT_RC(read_grow());
+        if (c->tail + grow[0] + 1024 > c->pool_cap) {
+            if (grow[0] + 1024 <= c->pool_cap / 4 * 3) {
+                SCOUT_RC(graph_compact(c, grow[0] + 1024, true));
             } else {
-                if (c->host_tail + grow > c->host_cap) {
-                    SCOUT_RC(host_compact(c));
-                    if (c->host_tail + grow > c->host_cap)
-                        return c->fail(SCOUT_E_CAPACITY, "tiered store: the host pool cannot take this batch's rows");
-                    SCOUT_RC(row_alloc(true));
-                }
-                c->dest_host = true;
+                c->batch_dest = 1;
                 c->host_batches++;
-                dest = elem_delta(c->host_pool, c->pool) + c->host_tail;
             }
+            SCOUT_RC(row_alloc(true, c->batch_dest == 2));
+            SCOUT_RC(read_grow());
+        }
+        const long long host_need = c->batch_dest == 1 ? grow[0] : grow[1];
+        if (c->host_tail + host_need > c->host_cap) {
+            SCOUT_RC(host_compact(c));
+            if (c->host_tail + host_need > c->host_cap)
+                return c->fail(SCOUT_E_CAPACITY, "tiered store: the host pool cannot take this batch's rows");
+            SCOUT_RC(row_alloc(true, c->batch_dest == 2));
+        }
+        const long long host_base = elem_delta(c->host_pool, c->pool) + c->host_tail;
+        if (c->batch_dest == 1) {
+            dest = host_base;
+        } else {
+            k_abs_off<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->d_old_row, c->d_ctr, (long long)c->pool_cap,
+                                                                    c->d_aff_len, c->d_aff_len2, (long long)c->tail,
+                                                                    host_base);
+            SCOUT_LAUNCH(c, "k_abs_off");
+            c->nlaunch += 1;
+            dest = 0;   // the offsets are absolute
         }
     }
     long long* dpos = (long long*)(sorted == c->d_keys ? c->d_keys_alt : c->d_keys);   // the free ping-pong half
@@ -1309,7 +1360,9 @@ int scout_graph_load_tiered(scout_ctx* c, int64_t n, const int64_t* off, const i
     SCOUT_RC(dev_alloc(c, (void**)&c->row, (size_t)n * sizeof(Row), "row table"));
     c->pool_cap = hbm_entries;
     SCOUT_RC(dev_alloc(c, (void**)&c->pool, (size_t)c->pool_cap * sizeof(int32_t), "element pool"));
-    c->host_cap = nnz + nnz / 2 + (1 << 20);
+    // after a host compaction the pool holds at most the live graph, and one batch adds at
+    // most a rewrite of every row it touches: 2 nnz (plus slack for insertions)
+    c->host_cap = 2 * nnz + (1 << 22);
     {
         void* hp = nullptr;
         cudaError_t e = cudaHostAlloc(&hp, (size_t)c->host_cap * 4, cudaHostAllocMapped | cudaHostAllocPortable);

@@ -1,5 +1,8 @@
 // io_host.cpp -- batch folders and initial-state files (core/cli_setup.h:64-131 and the
 // initial-state blocks of each reference main()).
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include "host.hpp"
 
 #include <algorithm>
@@ -70,11 +73,9 @@ static inline bool extract_int(const char*& p, const char* end, int64_t& out) {
 
 // parse_batch_file (cli_setup.h:87-103) minus classification: a line is kept if its first
 // two whitespace-separated tokens parse as ints; ids become 0-indexed; out-of-range ids and
-// self-loops are dropped.
-int parse_batch_text(const char* data, size_t len, int64_t n, std::vector<scout_edge>& out) {
-    out.clear();
-    const char* p = data;
-    const char* end = data + len;
+// self-loops are dropped. Large files are cut at line boundaries into one chunk per host
+// thread, parsed in parallel and concatenated in file order.
+static void parse_lines(const char* p, const char* end, int64_t n, std::vector<scout_edge>& out) {
     while (p < end) {
         const char* nl = (const char*)std::memchr(p, '\n', (size_t)(end - p));
         const char* le = nl ? nl : end;
@@ -88,6 +89,40 @@ int parse_batch_text(const char* data, size_t len, int64_t n, std::vector<scout_
         }
         p = nl ? nl + 1 : end;
     }
+}
+
+int parse_batch_text(const char* data, size_t len, int64_t n, std::vector<scout_edge>& out) {
+    out.clear();
+    const char* end = data + len;
+    int T = 1;
+#ifdef _OPENMP
+    if (len >= ((size_t)1 << 20)) T = std::max(1, std::min(omp_get_max_threads(), (int)(len >> 18)));
+#endif
+    if (T == 1) {
+        out.reserve(len / 12);
+        parse_lines(data, end, n, out);
+        return SCOUT_OK;
+    }
+    // chunk k starts after the first newline at or past k * len / T (chunk 0 at the start)
+    std::vector<const char*> cut((size_t)T + 1);
+    cut[0] = data;
+    cut[T] = end;
+    for (int k = 1; k < T; k++) {
+        const char* q = data + len * (size_t)k / (size_t)T;
+        const char* nl = (const char*)std::memchr(q, '\n', (size_t)(end - q));
+        cut[k] = nl ? nl + 1 : end;
+        if (cut[k] < cut[k - 1]) cut[k] = cut[k - 1];
+    }
+    std::vector<std::vector<scout_edge>> part((size_t)T);
+#pragma omp parallel for schedule(static, 1) num_threads(T)
+    for (int k = 0; k < T; k++) {
+        part[k].reserve((size_t)(cut[k + 1] - cut[k]) / 12);
+        parse_lines(cut[k], cut[k + 1], n, part[k]);
+    }
+    size_t total = 0;
+    for (auto& v : part) total += v.size();
+    out.reserve(total);
+    for (auto& v : part) out.insert(out.end(), v.begin(), v.end());
     return SCOUT_OK;
 }
 

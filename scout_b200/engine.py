@@ -270,6 +270,13 @@ class Context:
         self._c(LIB.scout_recompute_cc(self._h, C.byref(st)))
         return st.as_dict()
 
+    def seed(self, problem, source: int = 0) -> dict:
+        """Initial solution computed on the device from the current graph (greedy MIS and
+        colouring in vertex-id order, BFS levels from source, min-id components)."""
+        st = ScoutBatchStats()
+        self._c(LIB.scout_seed(self._h, _prob(problem), int(source), C.byref(st)))
+        return st.as_dict()
+
     def held_bytes(self) -> int:
         """Device bytes the context holds (every allocation counts against its budget)."""
         v = C.c_uint64()

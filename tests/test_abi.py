@@ -9,8 +9,8 @@ from conftest import ROOT
 
 from scout_b200 import _lib
 
-DECL = re.compile(r"^(?:int|int64_t|void|const char\s*\*|const int32_t\s*\*|const int64_t\s*\*)\s*\*?\s*(scout_\w+)\s*\(",
-                  re.M)
+DECL = re.compile(r"^(?:int|int64_t|void|const char\s*\*|const int32_t\s*\*|const int64_t\s*\*|scout_ctx\s*\*)"
+                  r"\s*\*?\s*(scout_\w+)\s*\(", re.M)
 
 
 def _declared():

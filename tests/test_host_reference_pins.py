@@ -181,3 +181,30 @@ def test_state_and_batch_writers_roundtrip(tmp_path):
     sb.write_batch_folder(str(tmp_path / "b"), e, 10, 2)
     got = np.concatenate([sb.parse_batch_file(str(tmp_path / "b" / f"{k}.mtx"), n) for k in (1, 2)])
     assert np.array_equal(got, e)
+
+
+def test_parallel_batch_parse_equals_serial(tmp_path):
+    """A batch file large enough to be parsed in parallel chunks gives the same edits, in file
+    order, as the line-by-line rule (malformed lines, out-of-range ids and self-loops dropped)."""
+    import numpy as np
+
+    import scout_b200 as sb
+    r = np.random.default_rng(4)
+    n = 5000
+    lines, want = [], []
+    for i in range(300000):
+        u, v = int(r.integers(0, n + 3)), int(r.integers(0, n + 3))
+        k = i % 97
+        if k == 0:
+            lines.append("garbage line")
+            continue
+        if k == 1:
+            lines.append(f"  {u + 1}\t{v + 1}  extra")
+        else:
+            lines.append(f"{u + 1} {v + 1}")
+        if 0 <= u < n and 0 <= v < n and u != v:
+            want.append((u, v))
+    p = tmp_path / "big.mtx"
+    p.write_text("\n".join(lines) + "\n")
+    got = sb.parse_batch_file(str(p), n)
+    assert np.array_equal(got, np.array(want, dtype=np.int32).reshape(-1, 2))
