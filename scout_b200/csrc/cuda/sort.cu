@@ -25,8 +25,10 @@ constexpr int SMALL_SORT_THREADS = 1024;
 // ---- one-sweep radix sort -------------------------------------------------------------------
 constexpr int OS_THREADS = 256;
 constexpr int OS_WARPS = OS_THREADS / WARP;
-constexpr int OS_STEPS = 16;                        // 32-key steps per warp
+constexpr int OS_STEPS = 16;                        // 32-key steps per warp (large sorts)
 constexpr int OS_TILE = OS_THREADS * OS_STEPS;      // 4096 keys per tile
+constexpr int OS_STEPS_SMALL = 4;                   // mid-size sorts: 1024-key tiles fill more SMs
+constexpr int OS_TILE_SMALL = OS_THREADS * OS_STEPS_SMALL;
 constexpr int OS_MAX_PASSES = 8;
 // control block in the sort buffer (32-bit words): [pass][256] histograms, then global digit
 // offsets; the done counter; the per-pass tile counters; the look-back entries (64-bit) follow
@@ -73,14 +75,16 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_hist(const unsigned long long
     if (threadIdx.x == 0) ctl[OS_DONE] = 0;
 }
 
-// One pass: stable scatter of every tile by the digit at `shift`. stamp tags this pass's
-// look-back entries (entries of earlier passes read as empty).
+// One pass: stable scatter of every tile of STEPS * 256 keys by the digit at `shift`. stamp
+// tags this pass's look-back entries (entries of earlier passes read as empty).
+template <int STEPS>
 __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const unsigned long long* __restrict__ src,
                                                         unsigned long long* __restrict__ dst, int64_t n, int pass,
                                                         unsigned int* __restrict__ ctl,
                                                         unsigned long long* __restrict__ lb, unsigned stamp,
                                                         int* __restrict__ err) {
-    __shared__ unsigned long long sk[OS_TILE];
+    constexpr int TILE = OS_THREADS * STEPS;
+    __shared__ unsigned long long sk[TILE];
     __shared__ unsigned int wh[OS_WARPS][SORT_RADIX];   // per-warp digit counts, then prefixes
     __shared__ unsigned int tot[SORT_RADIX], toff[SORT_RADIX];
     __shared__ long long gbase[SORT_RADIX];
@@ -91,14 +95,14 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const unsigned long long
     for (int j = 0; j < OS_WARPS; j++) wh[j][t] = 0;
     __syncthreads();
     const int tile = s_tile;
-    const int64_t t0 = (int64_t)tile * OS_TILE;
+    const int64_t t0 = (int64_t)tile * TILE;
     // each warp ranks its contiguous 512 keys, 32 at a time, in order (stable)
-    unsigned long long key[OS_STEPS];
-    unsigned short lr[OS_STEPS];
+    unsigned long long key[STEPS];
+    unsigned short lr[STEPS];
     const unsigned lt = (1u << l) - 1;
-    const int64_t wbase = t0 + (int64_t)w * (OS_STEPS * WARP);
+    const int64_t wbase = t0 + (int64_t)w * (STEPS * WARP);
 #pragma unroll
-    for (int s = 0; s < OS_STEPS; s++) {
+    for (int s = 0; s < STEPS; s++) {
         const int64_t i = wbase + s * WARP + l;
         const bool valid = i < n;
         key[s] = valid ? src[i] : ~0ull;
@@ -162,7 +166,7 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const unsigned long long
     __syncthreads();
     // stage the tile in digit order, then write it out: equal digits are contiguous runs
 #pragma unroll
-    for (int s = 0; s < OS_STEPS; s++) {
+    for (int s = 0; s < STEPS; s++) {
         const int64_t i = wbase + s * WARP + l;
         if (i < n) {
             const unsigned d = (unsigned)(key[s] >> shift) & 255u;
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(OS_THREADS) k_os_pass(const unsigned long long
         }
     }
     __syncthreads();
-    const int cnt = (int)min((int64_t)OS_TILE, n - t0);
+    const int cnt = (int)min((int64_t)TILE, n - t0);
     for (int j = t; j < cnt; j += OS_THREADS) {
         const unsigned long long k = sk[j];
         const unsigned d = (unsigned)(k >> shift) & 255u;
@@ -340,7 +344,7 @@ static unsigned next_stamp() {
 }
 
 int sort_reserve(scout_ctx* c, int64_t nkeys) {
-    const int64_t ntiles = (nkeys + OS_TILE - 1) / OS_TILE;
+    const int64_t ntiles = (nkeys + OS_TILE_SMALL - 1) / OS_TILE_SMALL;   // the most tiles a sort can have
     unsigned int* before = c->d_sort_hist;
     SCOUT_RC(dev_grow(c, &c->d_sort_hist, &c->cap_hist, OS_CTRL_WORDS + 2 * SORT_RADIX * ntiles, "sort look-back"));
     if (c->d_sort_hist != before)   // fresh memory: no stale look-back entry may match a stamp
@@ -369,7 +373,10 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
     }
     const int passes = (bits + 7) / 8;
     if (passes > OS_MAX_PASSES) return c->fail(SCOUT_E_INVALID, "sort keys wider than 64 bits");
-    const int64_t ntiles = (n + OS_TILE - 1) / OS_TILE;
+    // large tiles once they give every SM two of them, else small tiles
+    const bool small_tiles = (n + OS_TILE - 1) / OS_TILE < 2 * (int64_t)c->sm_count;
+    const int tile = small_tiles ? OS_TILE_SMALL : OS_TILE;
+    const int64_t ntiles = (n + tile - 1) / tile;
     SCOUT_RC(sort_reserve(c, n));
     unsigned int* ctl = c->d_sort_hist;
     unsigned long long* lb = (unsigned long long*)(ctl + OS_CTRL_WORDS);
@@ -382,8 +389,12 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
     unsigned long long* dst = alt;
     for (int p = 0; p < passes; p++) {
         const unsigned stamp = next_stamp();
-        k_os_pass<<<(unsigned)ntiles, OS_THREADS, 0, c->s_main>>>(src, dst, n, p, ctl, lb, stamp,
-                                                                  &c->d_ctr->sort_err);
+        if (small_tiles)
+            k_os_pass<OS_STEPS_SMALL><<<(unsigned)ntiles, OS_THREADS, 0, c->s_main>>>(src, dst, n, p, ctl, lb, stamp,
+                                                                                    &c->d_ctr->sort_err);
+        else
+            k_os_pass<OS_STEPS><<<(unsigned)ntiles, OS_THREADS, 0, c->s_main>>>(src, dst, n, p, ctl, lb, stamp,
+                                                                              &c->d_ctr->sort_err);
         SCOUT_LAUNCH(c, "k_os_pass");
         c->nlaunch += 1;
         unsigned long long* s = src; src = dst; dst = s;
