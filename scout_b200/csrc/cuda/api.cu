@@ -184,6 +184,8 @@ int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
     cudaMemset(c->d_ctr, 0, sizeof(DevCounters));
     cudaMemset(c->d_bar, 0, sizeof(GridBar));
     cudaMemset(c->d_flags, 0, 64);
+    std::memset(c->h_ctr, 0, sizeof(DevCounters));   // scout_sched_last before any repair reads it
+    std::memset(c->h_bar, 0, sizeof(GridBar));
     *out = c;
     return SCOUT_OK;
 }

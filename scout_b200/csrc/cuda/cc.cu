@@ -22,6 +22,8 @@
 // phases separated by the bounded grid barrier.
 #include "ctx.cuh"
 
+#include <atomic>
+
 namespace scout {
 
 constexpr int CC_THREADS = 256;
@@ -653,10 +655,12 @@ static int cc_launch(scout_ctx* c, const scout_sched* sched, int variant, const 
     p.mode_dev = mode_dev;
     p.ctr = c->d_ctr;
     p.bar = c->d_bar;
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is a per-device setting: once per device the process uses
+    static std::atomic<unsigned long long> attr_done{0};
+    const unsigned long long bit = 1ull << (c->device & 63);
+    if (!(attr_done.load() & bit)) {
         SCOUT_CU(c, cudaFuncSetAttribute(k_cc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CC_SMEM));
-        attr = true;
+        attr_done.fetch_or(bit);
     }
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_cc, CC_THREADS, args, CC_SMEM);

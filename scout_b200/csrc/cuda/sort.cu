@@ -361,10 +361,11 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
     if (n <= SMALL_SORT_MAX) {
         constexpr int NW = SMALL_SORT_THREADS / WARP;
         size_t smem = 2 * (size_t)n * sizeof(unsigned long long) + (size_t)(NW + 1) * SORT_RADIX * sizeof(unsigned);
-        static bool attr_set = false;
-        if (!attr_set) {
+        static std::atomic<unsigned long long> attr_done{0};   // per-device setting, once per device
+        const unsigned long long bit = 1ull << (c->device & 63);
+        if (!(attr_done.load() & bit)) {
             SCOUT_CU(c, cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-            attr_set = true;
+            attr_done.fetch_or(bit);
         }
         k_sort_small<<<1, SMALL_SORT_THREADS, smem, c->s_main>>>(keys, (int)n, bits);
         SCOUT_LAUNCH(c, "k_sort_small");

@@ -1,8 +1,8 @@
 """Records what the reference's own engines print on the bundled sample and on an R-MAT
 scale-16 stream, for every prefix of the batch stream. Needs a GPU and oracle/_ref/ (built by
-oracle/build_ref.sh from the reference sources); run on the GPU box:
+oracle/build_ref.sh from the reference sources); run on a machine with a B200:
 
-    python tests/golden/make_ref_engine_golden.py gpurun_out/ref_engines.json
+    python tests/golden/make_ref_engine_golden.py ref_engines.json
 
 and commit the JSON as tests/golden/ref_engines.json. Each entry holds the per-batch lines
 (edges, counters) and the final summary (solution measure, insertion/deletion breakdowns).
