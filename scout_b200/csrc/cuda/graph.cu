@@ -35,6 +35,12 @@ namespace scout {
 constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the long-row merge
 constexpr int SMALL_LEN = 2048;      // rows up to this length go to the short-row merge
 
+// A short row whose half-edits are all deletions is rewritten in place: its survivors only
+// move towards the row start, it keeps its start and capacity, and it takes no pool space.
+__host__ __device__ __forceinline__ bool in_place_row(long long insertions, int old_len) {
+    return insertions == 0 && old_len <= SMALL_LEN;
+}
+
 // ---------------------------------------------------------------------------------------
 // Staging
 // ---------------------------------------------------------------------------------------
@@ -238,14 +244,14 @@ __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict
             const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
             const Row r = row[aff[a]];
             old_row[a] = r;
-            alloc[a] = (long long)r.len + (sp - b0);
+            alloc[a] = in_place_row(sp - b0, r.len) ? 0 : (long long)r.len + (sp - b0);
             sm = r.len <= SMALL_LEN;
             ns = sm ? 0 : (r.len + SLICE - 1) / SLICE;
         }
         const int at = warp_append(ok && sm, &ctr->n_small);
         if (ok && sm) {
             small[at] = a;
-            small_len[at] = alloc[a] - (seg[3 * (int64_t)a + 1] - seg[3 * (int64_t)a]);   // the old length
+            small_len[at] = old_row[a].len;   // the merge balances its groups by old length
         }
         const int inc = warp_incl_scan_i(ns);
         int base = 0;
@@ -329,7 +335,8 @@ __global__ void k_plan_place(int32_t* __restrict__ pool, Row* __restrict__ row, 
         if (k == b0) {
             const long long p = sp - b0, q = e0 - sp;
             const long long nl = (long long)r.len + p - (E[e0] - E[sp]);
-            row[u] = Row{tail + off[a], (int)nl, (int)(r.len + p)};
+            row[u] = in_place_row(p, r.len) ? Row{r.start, (int)nl, r.cap}
+                                            : Row{tail + off[a], (int)nl, (int)(r.len + p)};
             nnz_delta += nl - r.len;
             bytes += 4 * (r.len + nl) + 8 * (p + q) + 16;
         }
@@ -382,7 +389,7 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
                 len = r.len;
                 ib = seg[3 * (int64_t)a];
                 p = (int)(seg[3 * (int64_t)a + 1] - ib);
-                ob = tail + off[a];
+                ob = in_place_row(p, len) ? st : tail + off[a];
             }
             s_cnt[w][lane] = 0;
             const int pin = warp_incl_scan_i(p);
@@ -413,6 +420,9 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
                     const long long sj = __shfl_sync(0xffffffffu, st, lo);
                     xx[u] = e < tot ? pool[sj + (e - ej)] : -1;
                 }
+                // rows rewritten in place: every load of this step precedes every store (a
+                // survivor's store lands at or before its load, and before any later load)
+                __syncwarp();
 #pragma unroll
                 for (int u = 0; u < U; u++) {
                     const int e0 = e00 + u * WARP;
