@@ -3,10 +3,11 @@
 //
 // Layout. row[v] = {start, len, cap} indexes the int32 pool; every row is kept sorted
 // ascending (a sorted multiset: a pair inserted twice in one batch appears twice, as the
-// reference's scratchpad appends it twice, core/FlashGraph.h:227-234). A batch never
-// rewrites a row in place: the merged row is appended at the pool tail and the descriptor
-// switched, so kernels reading other rows are never disturbed. The host compacts the pool
-// when the free space could not hold a full rewrite plus the batch.
+// reference's scratchpad appends it twice, core/FlashGraph.h:227-234). A row that gains
+// entries, or a long one, is merged into new space at the pool tail and its descriptor
+// switched; a short row whose half-edits are all deletions is compacted where it lies (its
+// survivors only move towards the row start; only the warp merging it touches it). The host
+// compacts the pool when the free space could not hold a full rewrite plus the batch.
 //
 // Batch merge (replaces DeltaOverlay::insertEdge / removeEdge + neighbors_into,
 // core/FlashGraph.h:227-265, done on the device for every affected row at once):
@@ -15,8 +16,8 @@
 //                     keys (u, op, v) and (v, op, u) per applied edit
 //   sort_keys         groups half-edits by vertex; inserts before deletes; neighbours sorted
 //   k_seg_heads/tails affected-vertex list and its key segments
-//   k_row_alloc       old descriptor, new space (old length + insertions), short-row list,
-//                     slices of long rows
+//   k_row_alloc       old descriptor, new space (old length + insertions; none for a short
+//                     row that only loses entries), short-row list, slices of long rows
 //   scan_i64          new rows' offsets in the pool
 //   k_plan_match      per deletion: the old entry it cancels (multiset rule); matched flags
 //   scan_i64          matched deletions before every half-edit
