@@ -51,8 +51,8 @@ def parse_args():
     ap.add_argument("--problems", default="bfs,coloring")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--ref-sample", type=int, default=20000, help="edits per batch timed in the reference arm")
-    ap.add_argument("--ref-timeout", type=float, default=150.0)
+    ap.add_argument("--ref-timeout", type=float, default=1500.0,
+                    help="seconds the reference programs may run in total (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--verbose", action="store_true", help="per-batch statistics on stderr")
     ap.add_argument("--model", default=os.path.join(ROOT, "scout_b200", "sched_model.npz"),
@@ -122,6 +122,26 @@ class Dist:
 # ---------------------------------------------------------------------------------------
 def batch_sizes(steps: int, warmup: int):
     return [SIZES[i % len(SIZES)] for i in range(warmup + steps)]
+
+
+def workload_config(a, n: int, nnz: int, sizes, problems, world: int) -> dict:
+    """The `config` object of both arms' lines (identical for the same arguments)."""
+    return {"workload": f"R-MAT scale {a.scale} EF16 (.57/.19/.19/.05) seed {a.seed}; "
+                        f"preferential 50/50 toggles; batch sizes {list(SIZES)} cycled; problems {problems}",
+            "vertices": n, "directed_entries": nnz, "graph_bytes": 4 * nnz + 8 * n,
+            "l2": "inputs larger than L2 (0.5 GB adjacency vs 126 MB L2); no flush",
+            "parallelism": f"replicas x{world}", "batch_sizes": list(sizes[a.warmup:])}
+
+
+def per_size_rates(edits, ms, sizes) -> dict:
+    """edge-updates/s per batch size, from per-batch (edits, ms) of the timed batches."""
+    out = {}
+    for z in sorted(set(sizes)):
+        e = sum(x for x, s_ in zip(edits, sizes) if s_ == z)
+        t = sum(x for x, s_ in zip(ms, sizes) if s_ == z)
+        if t > 0:
+            out[str(z)] = e / (t / 1e3)
+    return out
 
 
 def make_workload(scale: int, seed: int, stream_seed: int, sizes):
@@ -355,7 +375,9 @@ def scout_arm(a, dist):
                           "h2d_ms": sum(s["ms_h2d"] for s in per), "rounds": sum(s["rounds"] for s in per),
                           "changed": sum(s["commit_changed"] for s in per),
                           "scheduler": "learned" if p in model else "plain", "knobs": tuned.get(p, {}),
-                          "variants": [int(s["variant"]) for s in per]}
+                          "variants": [int(s["variant"]) for s in per],
+                          "per_size": per_size_rates([s["edits"] for s in per], [s["ms_step"] for s in per],
+                                                     sizes[a.warmup:a.warmup + len(per)])}
         if p in plain:
             pp, pe = plain[p]
             pdev = sum(s["ms_compact"] + s["ms_update"] + s["ms_repair"] for s in pp)
@@ -393,11 +415,7 @@ def scout_arm(a, dist):
         "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * e2e_s / max(n_steps, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT + preferential toggle stream)",
-        "config": {"workload": f"R-MAT scale {a.scale} EF16 (.57/.19/.19/.05) seed {a.seed}; "
-                               f"preferential 50/50 toggles; batch sizes {list(SIZES)} cycled; problems {problems}",
-                   "vertices": int(g.n), "directed_entries": int(g.nnz), "graph_bytes": int(4 * g.nnz + 8 * g.n),
-                   "l2": "inputs larger than L2 (0.5 GB adjacency vs 126 MB L2); no flush",
-                   "parallelism": f"replicas x{dist.world}", "batch_sizes": sizes[a.warmup:]},
+        "config": workload_config(a, int(g.n), int(g.nnz), sizes, problems, dist.world),
         "p50_batch_ms": float(np.percentile(all_ms, 50)), "p99_batch_ms": float(np.percentile(all_ms, 99)),
         "per_problem": per_problem,
         "e2e": {"value": edits_all / e2e_s if e2e_s else None, "unit": "edge-updates/s",
@@ -619,66 +637,120 @@ def multi_stream(a, device, model, tuned):
 # ---------------------------------------------------------------------------------------
 # reference arm: the reference's own programs (oracle/_ref, compiled from its sources)
 # ---------------------------------------------------------------------------------------
-BATCH_RE = re.compile(r"^Batch (\d+)/(\d+) \| edges=(\d+) \| time=([0-9.]+)ms")
+BATCH_RE = re.compile(r"^Batch (\d+)/(\d+) \| edges=(\d+) \| time=([0-9.]+)ms(.*)$")
+FALLBACK_RE = re.compile(r"fallback=(\d+)")
+DEFERRED_RE = re.compile(r"^\[DEFERRED FALLBACK\] done in ([0-9.]+) ms")
+
+
+def reference_workload(a, sizes):
+    """The scout arm's workload rebuilt without this package's library: the numpy
+    restatement of the generator (byte-identical, tests/test_gen_oracle.py) and the oracle's
+    initial-state solvers (BFS from vertex 0, greedy smallest-free colouring in id order,
+    min-id components, greedy MIS in id order)."""
+    from oracle import gen_oracle as go
+    from oracle import oracle as orc
+    off, adj = go.gen_rmat(a.scale, 16, seed=a.seed)
+    s = go.gen_stream(off, adj, go.STREAM_PREFERENTIAL, sum(sizes), 0.5, seed=1000 + a.seed)
+    bounds = np.cumsum([0] + list(sizes))
+    batches = [s[bounds[i]:bounds[i + 1]] for i in range(len(sizes))]
+    init = {"bfs": lambda: orc.gt_bfs(off, adj, 0), "coloring": lambda: orc.gt_greedy_color(off, adj),
+            "cc": lambda: orc.gt_cc(off, adj), "mis": lambda: orc.gt_greedy_mis(off, adj)}
+    return off, adj, batches, init
+
+
+def run_reference_program(path, egr, state, bdir, nb, gpu, timeout, cwd):
+    """Runs one reference binary over the batch folder; returns (per-batch rows, deferred
+    catch-up ms, complete, wall seconds). A row is (batch, edits, ms, fallback count)."""
+    cmd = [path, egr, state, bdir, str(nb), str(gpu)]
+    env = dict(os.environ, SCOUT_SKIP_COMPACTION="1")
+    t0 = time.perf_counter()
+    complete = True
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, env=env, cwd=cwd)
+        out = r.stdout
+        complete = r.returncode == 0
+    except subprocess.TimeoutExpired as e:
+        out = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
+        complete = False
+    wall = time.perf_counter() - t0
+    rows, deferred = [], 0.0
+    for line in out.splitlines():
+        m = BATCH_RE.match(line)
+        if m:
+            fb = FALLBACK_RE.search(m.group(5))
+            rows.append((int(m.group(1)), int(m.group(3)), float(m.group(4)), int(fb.group(1)) if fb else 0))
+            continue
+        d = DEFERRED_RE.match(line)
+        if d:
+            deferred += float(d.group(1))
+    complete = complete and len(rows) == nb
+    return rows, deferred, complete, wall
 
 
 def reference_arm(a, dist):
-    import scout_b200 as sb
+    """The unmodified reference programs (src/<problem>/scout_<problem>.cu built for sm_100a
+    by oracle/build_ref.sh) on exactly the scout arm's workload: the same graph written as a
+    narrow .egr, the same warm-up + timed batches as a batch folder, the same initial states.
+    Each program runs the whole folder; the timed batches are those after the warm-up, their
+    time from the program's own per-batch `time=` lines. The end-of-stream catch-up traversal
+    (SCOUT_DEFER_FALLBACK, the reference default) is what makes the deferred batches exact, so
+    its time is charged to the timed batches in proportion to their deferred cascades."""
     sizes = batch_sizes(a.steps, a.warmup)
     problems = [p.strip() for p in a.problems.split(",") if p.strip()]
-    g, off, adj, batches, init = make_workload(a.scale, a.seed, 1000 + a.seed, sizes)
-    sample = [b[: a.ref_sample] for b in batches]
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
-    have = all(os.path.exists(os.path.join(ref_dir, f"scout_{p}")) for p in problems)
     cores = os.cpu_count()
-    if not have:
-        # the oracle port of the reference engine on the host cores (single thread)
-        cb = cpu_baseline(problems, off, adj, init, sample, a.cpu_seconds * 2)
-        return {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "edge-updates/s",
-                "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
-                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "edge-updates/s", "h2d_bytes_per_step": 0,
-                                            "d2h_bytes_per_step": 0}}
+    t_gen = time.perf_counter()
+    off, adj, batches, init = reference_workload(a, sizes)
+    n, nnz = len(off) - 1, int(off[-1])
+    config = workload_config(a, n, nnz, sizes, problems, dist.world)
+    base = {"impl": "reference", "metric": METRIC, "unit": "edge-updates/s", "n_gpus": dist.world,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "dtype": "int32",
+            "data": "synthetic (seeded R-MAT + preferential toggle stream)", "config": config}
+    missing = [p for p in problems if not os.path.exists(os.path.join(ref_dir, f"scout_{p}"))]
+    if missing:
+        return dict(base, unavailable=f"reference programs not built for {missing} (oracle/build_ref.sh needs the "
+                                      f"reference sources)")
+    from oracle import gen_oracle as go
     per_problem = {}
     edits_t = ms_t = 0.0
+    complete = True
     with tempfile.TemporaryDirectory() as td:
         egr = os.path.join(td, "g.egr")
-        sb.write_egr(egr, off, adj, wide=False)
+        go.write_egr_narrow(egr, off, adj)
         bdir = os.path.join(td, "batches")
-        os.makedirs(bdir)
-        for k, b in enumerate(sample):
-            sb.write_batch_folder(os.path.join(td, "one"), b, len(b), 1)
-            os.replace(os.path.join(td, "one", "1.mtx"), os.path.join(bdir, f"{k + 1}.mtx"))
+        go.write_batch_folder(bdir, batches)
+        gen_s = time.perf_counter() - t_gen
+        budget = a.ref_timeout
         for p in problems:
             st = os.path.join(td, f"{p}.txt")
-            sb.write_state(st, p, init[p])
-            cmd = [os.path.join(ref_dir, f"scout_{p}"), egr, st, bdir, str(len(sample)), str(dist.local)]
-            env = dict(os.environ, SCOUT_SKIP_COMPACTION="1")
-            try:
-                r = subprocess.run(cmd, capture_output=True, text=True, timeout=a.ref_timeout, env=env, cwd=td)
-                out = r.stdout
-            except subprocess.TimeoutExpired as e:
-                out = e.stdout.decode() if isinstance(e.stdout, bytes) else (e.stdout or "")
-            rows = [BATCH_RE.match(l) for l in out.splitlines()]
-            rows = [(int(m.group(1)), int(m.group(3)), float(m.group(4))) for m in rows if m]
+            go.write_state(st, p, init[p]())
+            rows, deferred, ok, wall = run_reference_program(os.path.join(ref_dir, f"scout_{p}"), egr, st, bdir,
+                                                             len(batches), dist.local, max(60.0, budget), td)
+            budget -= wall
+            complete = complete and ok
             timed = [r for r in rows if r[0] > a.warmup]
+            fb_all = sum(r[3] for r in rows)
+            fb_timed = sum(r[3] for r in timed)
+            share = deferred * (fb_timed / fb_all) if fb_all else 0.0
             e = sum(r[1] for r in timed)
-            ms = sum(r[2] for r in timed)
+            ms = sum(r[2] for r in timed) + share
             per_problem[p] = {"edge_updates_per_s": e / (ms / 1e3) if ms else None, "batches_timed": len(timed),
-                              "edits": e, "ms": ms}
+                              "edits": e, "ms": ms, "deferred_catch_up_ms": deferred,
+                              "deferred_charged_ms": share, "complete": ok, "program_wall_s": wall,
+                              "per_size": per_size_rates([r[1] for r in timed], [r[2] for r in timed],
+                                                         [sizes[r[0] - 1] for r in timed])}
             edits_t += e
             ms_t += ms
     val = edits_t / (ms_t / 1e3) if ms_t else None
-    return {"impl": "reference", "metric": METRIC, "value": val, "unit": "edge-updates/s", "n_gpus": dist.world,
-            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "dtype": "int32",
-            "data": "synthetic (seeded R-MAT + preferential toggle stream)",
-            "config": {"workload": f"R-MAT scale {a.scale} EF16 seed {a.seed}; preferential 50/50 toggles; "
-                                   f"first {a.ref_sample} toggles of each batch; problems {problems}"},
-            "per_problem": per_problem,
-            "cpu_baseline": {"value": val, "unit": "edge-updates/s", "cores": cores, "kind": "reference",
-                             "sample": f"reference binaries (src/*/scout_*.cu built for sm_100a, OpenMP host "
-                                       f"fetch) on the first {a.ref_sample} toggles of each batch; their own "
-                                       f"per-batch time= lines, warm-up batches excluded"},
-            "e2e": {"value": val, "unit": "edge-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    sample = (f"reference programs (src/*/scout_*.cu built for sm_100a, OpenMP host fetch on {cores} threads) on "
+              f"the full workload: {len(batches)} batches, the last {a.steps} timed from their own per-batch "
+              f"time= lines plus the charged share of the deferred catch-up; inputs generated in {gen_s:.0f} s "
+              f"by the oracle's numpy generator")
+    return dict(base, value=val, ms_per_step=ms_t / max(1, a.steps * len(problems)), complete=complete,
+                per_problem=per_problem,
+                cpu_baseline={"value": val, "unit": "edge-updates/s", "cores": cores, "kind": "reference",
+                              "sample": sample},
+                e2e={"value": val, "unit": "edge-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
 
 
 def main():

@@ -306,13 +306,14 @@ int scout_host_free(void* p);
  * the caller already holds in device memory (d_off: n + 1 int64 offsets, d_adj: int32
  * neighbours), written to the caller's device buffer d_level (n int32), on the caller's
  * stream (a cudaStream_t, NULL for the default stream); returns when the levels are ready.
- * It allocates nothing: for callers that cannot call cudaMalloc (code running while a CUDA
- * graph is being captured, runtimes whose device memory belongs to another allocator or a
- * fixed arena, real-time loops that must stay off the driver's allocator). Its working
+ * It allocates nothing: for callers that cannot call cudaMalloc (runtimes whose device
+ * memory belongs to another allocator or a fixed arena, real-time loops that must stay off
+ * the driver's allocator). Its working
  * buffers live in one static device array of 8 MB that every GPU loading the library keeps
  * until the process exits, which bounds n to 1,048,576 vertices; larger graphs are refused
- * with SCOUT_E_CAPACITY. The first call on a device looks up that array's device address,
- * so make it before any stream capture. All calls share the array: calls that overlap on
+ * with SCOUT_E_CAPACITY. The first call on a device looks up that array's device address
+ * (again after the device's context is recreated), so make the first call before any stream
+ * capture. All calls share the array: calls that overlap on
  * the GPU (two host threads, or two streams) race and must be serialised by the caller.
  * No context is involved; errors are reported through scout_last_error(NULL). */
 int scout_bfs_levels_noalloc(const int64_t* d_off, const int32_t* d_adj, int64_t n, int32_t source,

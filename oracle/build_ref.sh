@@ -10,8 +10,9 @@
 #   ref_core_driver               oracle/ref_core_driver.cpp over core/*.h
 # Set FORCE=1 to rebuild. The engines need nvcc and take a while; the rest is seconds.
 set -euo pipefail
-REF="${SCOUT_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# the reference tree: $SCOUT_REFERENCE_DIR, else `reference` beside the repository root
+REF="${SCOUT_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 FORCE="${FORCE:-0}"
 NVCC="${NVCC:-nvcc}"

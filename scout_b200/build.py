@@ -116,10 +116,16 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
+def reference_dir() -> str:
+    """The reference tree: $SCOUT_REFERENCE_DIR, else a `reference` directory beside the
+    repository root (absent on machines that only run the prebuilt files)."""
+    return os.environ.get("SCOUT_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
+
+
 def build_reference(force: bool = False) -> None:
     """Compiles the reference's binaries from its own sources (checker only)."""
     script = os.path.join(ORACLE, "build_ref.sh")
-    ref = os.environ.get("SCOUT_REFERENCE_DIR", "/root/reference")
+    ref = reference_dir()
     if not (os.path.exists(script) and os.path.isdir(ref)):
         return
     env = dict(os.environ, SCOUT_REFERENCE_DIR=ref, FORCE="1" if force else "0")

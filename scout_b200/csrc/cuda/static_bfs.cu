@@ -1,17 +1,20 @@
 // static_bfs.cu -- BFS levels over a caller-owned device CSR without any allocation.
 //
-// For callers that cannot allocate device memory themselves: code running while a CUDA graph
-// is being captured (cudaMalloc is not capturable), processes whose device memory is owned
-// by another allocator or a fixed arena (a runtime embedding this library through cgo/JNI,
-// for instance), and real-time loops that must not hit the driver's allocator. They pass the
-// graph and the output in device memory they already hold; every working buffer of the
-// traversal (two frontier queues, counters, the grid barrier) lives in the file-scope array
-// g_bfs_scratch below, which each device that loads the library keeps until exit.
+// For callers that cannot allocate device memory themselves: processes whose device memory is
+// owned by another allocator or a fixed arena (a runtime embedding this library through
+// cgo/JNI, for instance, whose memory manager has already claimed the device), and real-time
+// loops that must not enter the driver's allocator. They pass the graph and the output in
+// device memory they already hold; every working buffer of the traversal (two frontier
+// queues, counters, the grid barrier) lives in the file-scope array g_bfs_scratch below,
+// which each device that loads the library keeps until exit.
 //
 // The device code names g_bfs_scratch directly; host code only ever uses the device address
-// cudaGetSymbolAddress returns for it (the symbol itself is a host-side stand-in).
+// cudaGetSymbolAddress returns for it (the symbol itself is a host-side stand-in). That
+// address is looked up once per device and context: a call after the device's context was
+// torn down and recreated (cudaDeviceReset) looks it up again.
 #include "ctx.cuh"
 
+#include <cuda.h>
 #include <mutex>
 
 namespace scout {
@@ -70,7 +73,29 @@ k_static_bfs(const int64_t* __restrict__ off, const int32_t* __restrict__ adj, i
 
 static std::mutex g_setup_mu;
 static int32_t* g_scratch_dev[64];   // device address of g_bfs_scratch, per device ordinal
+static CUcontext g_scratch_ctx[64];  // the context that address belongs to
 static bool g_scratch_ready[64];
+
+// The calling thread's current context, through the driver entry point the runtime exposes
+// (no link-time dependency on the driver library); null when it cannot be queried.
+static CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (Fn)p;
+        else
+            cudaGetLastError();
+        looked = true;
+    }
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 }  // namespace scout
 
@@ -89,14 +114,17 @@ extern "C" int scout_bfs_levels_noalloc(const int64_t* d_off, const int32_t* d_a
     if (e != cudaSuccess || dev < 0 || dev >= 64) return cuda_fail(nullptr, e, "cudaGetDevice");
     int32_t* scratch = nullptr;
     {
-        // One-time set-up per device, with that device current: the device address of the
-        // static array (the first call should therefore come before any stream capture).
+        // One-time set-up per device (and per context of it), with that device current: the
+        // device address of the static array. The first call on a device does it, so that call
+        // should come before any stream capture.
         std::lock_guard<std::mutex> g(g_setup_mu);
-        if (!g_scratch_ready[dev]) {
+        const CUcontext cur = current_context();
+        if (!g_scratch_ready[dev] || g_scratch_ctx[dev] != cur) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_bfs_scratch);
             if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetSymbolAddress(g_bfs_scratch)");
             g_scratch_dev[dev] = (int32_t*)p;
+            g_scratch_ctx[dev] = current_context();
             g_scratch_ready[dev] = true;
         }
         scratch = g_scratch_dev[dev];

@@ -1,6 +1,7 @@
 """Generates the committed golden fixtures from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference) after
+Run where the reference tree is available ($SCOUT_REFERENCE_DIR, else `reference` beside the
+repository root) after
 `bash oracle/build_ref.sh`:
 
     python tests/golden/make_golden.py
@@ -32,7 +33,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF = os.environ.get("SCOUT_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("SCOUT_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
 
 

@@ -1,9 +1,10 @@
 """The allocation-free BFS entry point (scout_bfs_levels_noalloc) gives the same levels as the
-context-based full recompute (scout_recompute_bfs), call after call.
+context-based full recompute (scout_recompute_bfs) and as the oracle's from-scratch BFS, call
+after call.
 
-Callers of this entry point cannot allocate device memory themselves (stream capture in
-progress, a foreign allocator owns the device memory, real-time code); the library keeps its
-working buffers in a static device array instead, so repeated calls reuse it. This file is
+Callers of this entry point cannot allocate device memory themselves (a foreign allocator or
+fixed arena owns the device memory, real-time code); the library keeps its working buffers in
+a static device array instead, so repeated calls reuse it. This file is
 collected last so a failure here leaves every other test already run; it passes alone in a
 fresh process too.
 """
@@ -13,6 +14,7 @@ import numpy as np
 import pytest
 
 import scout_b200 as sb
+from oracle import oracle as orc
 from scout_b200._lib import LIB
 
 pytestmark = pytest.mark.gpu
@@ -48,12 +50,15 @@ def test_noalloc_bfs_matches_recompute_twice(sample_graph, rmat16):
     for name, off, adj, src in _graphs(sample_graph, rmat16):
         n = len(off) - 1
         want = _levels_via_context(off, adj, src)
+        assert np.array_equal(want, orc.gt_bfs(off, adj, src)), f"{name}: the context recompute differs"
         d_off = torch.from_numpy(np.ascontiguousarray(off, dtype=np.int64)).cuda()
         d_adj = torch.from_numpy(np.ascontiguousarray(adj, dtype=np.int32)).cuda()
         d_lev = torch.full((n,), 12345, dtype=torch.int32, device="cuda")
+        free0 = torch.cuda.mem_get_info()[0]
         for call in range(2):   # the static array keeps the previous call's contents
             got = _levels_noalloc(torch, d_off, d_adj, n, src, d_lev)
             assert np.array_equal(got, want), f"{name}: call {call + 1} differs"
+        assert torch.cuda.mem_get_info()[0] == free0, f"{name}: device memory was allocated"
 
 
 def test_noalloc_refuses_oversized_graphs():
