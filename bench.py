@@ -338,6 +338,38 @@ def cpu_baseline(problems, off, adj, init, batches, seconds):
                       + "; ".join(parts)}
 
 
+def cpu_recompute_baseline(problems, off, adj, batches, warmup, seconds):
+    """All-core from-scratch recompute on the host (oracle/cpu_recompute.cpp, OpenMP): the
+    oracle's graph follows the stream with the toggle rule, and after each timed batch of the
+    sample every problem's solution is recomputed from scratch (parallel BFS, CAS union-find;
+    greedy colouring and MIS are sequential by definition). edge-updates/s = the sample's edits
+    per problem / the recompute seconds (the graph updates themselves are not charged)."""
+    from oracle import oracle as orc
+    g = orc.Graph(off, adj)
+    for b in batches[:warmup]:
+        g.toggle_batch(b)
+    per = {p: [0, 0.0] for p in problems}
+    t0 = time.perf_counter()
+    k = 0
+    for b in batches[warmup:]:
+        if time.perf_counter() - t0 > seconds and k >= 1:
+            break
+        g.toggle_batch(b)
+        o, a_ = g.csr()
+        for p in problems:
+            _, t = orc.cpu_recompute(p, o, a_, 0)
+            per[p][0] += len(b)
+            per[p][1] += t
+        k += 1
+    edits = sum(v[0] for v in per.values())
+    secs = sum(v[1] for v in per.values())
+    return {"value": edits / secs if secs else None, "unit": "edge-updates/s", "cores": orc.cpu_threads(),
+            "kind": "from-scratch recompute",
+            "per_problem": {p: (v[0] / v[1] if v[1] else None) for p, v in per.items()},
+            "sample": f"the first {k} timed batches of the same stream ({per[problems[0]][0]} toggles), each "
+                      f"followed by a from-scratch recompute of {problems} on {orc.cpu_threads()} threads"}
+
+
 def scout_arm(a, dist):
     import scout_b200 as sb
     sizes = batch_sizes(a.steps, a.warmup)
@@ -432,6 +464,7 @@ def scout_arm(a, dist):
     }
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(problems, off, adj, init, batches, a.cpu_seconds)
+        line["cpu_recompute"] = cpu_recompute_baseline(problems, off, adj, batches, a.warmup, a.cpu_seconds)
     if dist.world == 1 and not a.no_multi:
         del g, off, adj, batches, init
         line["multi_stream"] = multi_stream(a, device, model, tuned)

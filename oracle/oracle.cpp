@@ -671,6 +671,22 @@ int64_t orc_graph_row(void* g, int v, int32_t* out, int64_t cap) {
     for (int64_t i = 0; i < (int64_t)row.size() && i < cap; i++) out[i] = row[i];
     return (int64_t)row.size();
 }
+// One batch of toggles (u, v pairs): each pair is classified against the graph as it stood
+// before the batch (cli_setup.h:87-103), then applied; self-loops and out-of-range ids skipped.
+void orc_graph_toggle_batch(void* gp, const int32_t* uv, int64_t m) {
+    OGraph* g = (OGraph*)gp;
+    std::vector<char> ins((size_t)m, 0);
+    for (int64_t i = 0; i < m; i++) {
+        const int u = uv[2 * i], v = uv[2 * i + 1];
+        if (u == v || u < 0 || v < 0 || u >= g->n || v >= g->n) { ins[i] = 2; continue; }
+        ins[i] = g->is_adjacent(u, v) ? 0 : 1;
+    }
+    for (int64_t i = 0; i < m; i++) {
+        if (ins[i] == 2) continue;
+        if (ins[i]) g->insert_edge(uv[2 * i], uv[2 * i + 1]);
+        else g->remove_edge(uv[2 * i], uv[2 * i + 1]);
+    }
+}
 int64_t orc_graph_nnz(void* gp) {
     OGraph* g = (OGraph*)gp;
     int64_t s = 0;

@@ -23,10 +23,18 @@ _i32p = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
 
 
+SOURCES = ("oracle.cpp", "cpu_recompute.cpp")
+
+
 def _load() -> C.CDLL:
-    src = os.path.join(_HERE, "oracle.cpp")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
-        subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", src, "-o", LIB_PATH])
+    srcs = [os.path.join(_HERE, f) for f in SOURCES]
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(s) for s in srcs):
+        objs = [LIB_PATH + f".{i}.o" for i in range(len(srcs))]
+        for src, obj in zip(srcs, objs):   # OpenMP at compile time, libgomp named at link time
+            subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-c", src, "-o", obj])
+        subprocess.check_call(["g++", "-shared"] + objs + ["-l:libgomp.so.1", "-o", LIB_PATH])
+        for obj in objs:
+            os.remove(obj)
     lib = C.CDLL(LIB_PATH)
     sig = {
         "orc_graph_new": (C.c_void_p, [C.c_int64, _i64p, _i32p]),
@@ -38,6 +46,9 @@ def _load() -> C.CDLL:
         "orc_graph_row": (C.c_int64, [C.c_void_p, C.c_int, _i32p, C.c_int64]),
         "orc_graph_nnz": (C.c_int64, [C.c_void_p]),
         "orc_graph_export": (None, [C.c_void_p, _i64p, _i32p]),
+        "orc_graph_toggle_batch": (None, [C.c_void_p, _i32p, C.c_int64]),
+        "orc_cpu_recompute": (C.c_double, [C.c_int, C.c_int64, _i64p, _i32p, C.c_int32, C.c_int, _i32p]),
+        "orc_cpu_threads": (C.c_int, []),
         "orc_engine_new": (C.c_void_p, [C.c_int, C.c_int64, _i64p, _i32p, _i32p, C.c_int64, C.c_int]),
         "orc_engine_free": (None, [C.c_void_p]),
         "orc_engine_batch": (None, [C.c_void_p, _i32p, C.c_int64]),
@@ -102,6 +113,11 @@ class Graph:
         out = np.zeros(max(d, 1), dtype=np.int32)
         LIB.orc_graph_row(self._h, v, _p32(out), len(out))
         return out[:d]
+
+    def toggle_batch(self, edges):
+        """Applies a batch of toggles, each classified against the pre-batch graph."""
+        e = np.ascontiguousarray(edges, dtype=np.int32).reshape(-1, 2)
+        LIB.orc_graph_toggle_batch(self._h, _p32(e), len(e))
 
     def csr(self):
         nnz = LIB.orc_graph_nnz(self._h)
@@ -209,3 +225,19 @@ def canonical_labels(labels) -> np.ndarray:
     _, first = np.unique(lab, return_index=True)
     mapping = dict(zip(lab[first].tolist(), first.tolist()))
     return np.array([mapping[x] for x in lab.tolist()], dtype=np.int32)
+
+
+# ---- all-core from-scratch recompute (a benchmark baseline, oracle/cpu_recompute.cpp) ---------
+RECOMPUTE = {"mis": 0, "coloring": 1, "bfs": 2, "cc": 3}
+
+
+def cpu_recompute(problem: str, off, adj, source: int = 0, threads: int = 0):
+    """(solution, seconds) of a from-scratch recompute on `threads` host threads (0: all)."""
+    off, adj = _csr(off, adj)
+    out = np.zeros(len(off) - 1, dtype=np.int32)
+    t = LIB.orc_cpu_recompute(RECOMPUTE[problem], len(off) - 1, _p64(off), _p32(adj), source, threads, _p32(out))
+    return out, float(t)
+
+
+def cpu_threads() -> int:
+    return int(LIB.orc_cpu_threads())

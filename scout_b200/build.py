@@ -109,10 +109,16 @@ def build_cli(force: bool = False) -> list[str]:
 
 
 def build_oracle(force: bool = False) -> str:
-    src = os.path.join(ORACLE, "oracle.cpp")
+    srcs = [os.path.join(ORACLE, f) for f in ("oracle.cpp", "cpu_recompute.cpp")]
     out = os.path.join(ORACLE, "liboracle.so")
-    if force or _stale(out, [src]):
-        _run([CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", src, "-o", out])
+    if force or _stale(out, srcs):
+        os.makedirs(OBJDIR, exist_ok=True)
+        objs = []
+        for src in srcs:   # OpenMP at compile time, libgomp named at link time
+            obj = os.path.join(OBJDIR, "oracle_" + os.path.basename(src) + ".o")
+            _run([CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-c", src, "-o", obj])
+            objs.append(obj)
+        _run([CXX, "-shared"] + objs + ["-l:libgomp.so.1", "-o", out])
     return out
 
 
