@@ -104,6 +104,12 @@ typedef struct scout_batch_stats {
                              incremental, 1 recompute of every class; others 0)     */
     double  ms_compact;   /* device: pool compaction before the merge (0 when none ran) */
     int64_t compactions;  /* pool compactions of the context so far                   */
+    int64_t ins_effective; /* BFS: insertions that lowered a level (the reference's
+                              "repaired"); CC: insertions that merged two components
+                              ("merged"); coloring: same-colour insertions             */
+    int64_t del_effective; /* BFS: deletions of a shortest-path tree edge (the reference's
+                              local + fallback); CC: deletions whose local search split
+                              a component (the reference's "definitive_split")        */
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;

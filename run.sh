@@ -7,8 +7,9 @@
 #   ./run.sh --problem=mis|coloring|bfs|cc --sample
 #
 # --num-batches defaults to the number of *.mtx files in the batch folder; --gpu to 0.
-# Environment: NVCC (compiler used by the build), SCOUT_SKIP_COMPACTION=1 (mis: keep the
-# .egr untouched), SCOUT_DEVICE_BUDGET_GB (cap on the engine's HBM use).
+# Environment: NVCC (compiler used by the build), SCOUT_ARCH_FLAG (accepted; the engine is
+# written for sm_100a and always built for it), SCOUT_SKIP_COMPACTION=1 (mis: keep the .egr
+# untouched), SCOUT_DEVICE_BUDGET_GB (cap on the engine's HBM use).
 set -euo pipefail
 
 SCRIPT_DIR="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -28,6 +29,8 @@ Usage: $0 --problem=mis|coloring|bfs|cc --graph=<graph.egr> --init=<initial_stat
 
 Environment overrides:
   NVCC                      nvcc binary used by the build (default: nvcc on PATH)
+  SCOUT_ARCH_FLAG           accepted for compatibility; the kernels are written for sm_100a
+                            (B200) and always built with -gencode arch=compute_100a,code=sm_100a
   SCOUT_SKIP_COMPACTION=1   mis: skip the end-of-run .egr compaction step
   SCOUT_DEVICE_BUDGET_GB    cap on the HBM the engine may use
 EOF
@@ -76,6 +79,9 @@ if [ -z "$NUM_BATCHES" ]; then
     NUM_BATCHES=$(find "$BATCH" -maxdepth 1 -name '*.mtx' | wc -l | tr -d ' ')
 fi
 
+if [ -n "${SCOUT_ARCH_FLAG:-}" ] && [ "$SCOUT_ARCH_FLAG" != "-arch=sm_100a" ]; then
+    echo "Note: SCOUT_ARCH_FLAG=$SCOUT_ARCH_FLAG ignored; the engine is built for sm_100a" >&2
+fi
 BIN="$SCRIPT_DIR/bin/scout_$PROBLEM"
 if [ ! -x "$BIN" ]; then
     echo "Building $BIN ..."

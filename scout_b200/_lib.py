@@ -40,7 +40,7 @@ class ScoutBatchStats(C.Structure):
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
                 ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
                 ("phase_ms", C.c_double * 4), ("variant", C.c_int64), ("ms_compact", C.c_double),
-                ("compactions", C.c_int64)]
+                ("compactions", C.c_int64), ("ins_effective", C.c_int64), ("del_effective", C.c_int64)]
 
     def as_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("reserved", "phase_ms")}

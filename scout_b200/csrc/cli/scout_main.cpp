@@ -165,7 +165,9 @@ int main(int argc, char** argv) {
     if ((int)paths.size() > num_batches) paths.resize((size_t)std::max(num_batches, 0));
 
     // Parse every batch; MIS classifies all of them against the base graph up front
-    // (scout_mis.cu:835-842) and removes repeated identical lines inside a batch.
+    // (scout_mis.cu:835-842), on the device (a binary search in the sorted HBM rows instead of
+    // the reference's linear base-row scan, FlashGraph.h:356-366), after removing repeated
+    // identical lines inside a batch.
     std::vector<std::vector<scout_edge>> batches;
     std::vector<std::vector<uint8_t>> ops;
     for (auto& p : paths) {
@@ -180,13 +182,15 @@ int main(int argc, char** argv) {
             std::unordered_set<uint64_t> seen;
             std::vector<scout_edge> kept;
             for (auto& x : b) {
-                int a = scout_hgraph_is_adjacent(h, x.u, x.v);
                 uint64_t key = ((uint64_t)(uint32_t)x.u << 32) | (uint32_t)x.v;
-                if (!seen.insert(key).second) continue;
-                kept.push_back(x);
-                op.push_back(a ? SCOUT_OP_DELETE : SCOUT_OP_INSERT);
+                if (seen.insert(key).second) kept.push_back(x);
             }
             b.swap(kept);
+            std::vector<uint8_t> ins(b.size());
+            if (!b.empty() && scout_classify(ctx, b.data(), (int64_t)b.size(), ins.data()) != SCOUT_OK)
+                die("classification failed", scout_last_error(ctx));
+            op.resize(b.size());
+            for (size_t k = 0; k < b.size(); k++) op[k] = ins[k] == 1 ? SCOUT_OP_INSERT : SCOUT_OP_DELETE;
         }
         batches.push_back(std::move(b));
         ops.push_back(std::move(op));
@@ -195,7 +199,9 @@ int main(int argc, char** argv) {
     std::unordered_set<int32_t> touched;
     const bool dump_touched = std::getenv("SCOUT_DUMP_TOUCHED") != nullptr;
     double proc_ms = 0;
-    long long tot_ins = 0, tot_del = 0, tot_conf = 0, tot_rounds = 0;
+    long long tot_ins = 0, tot_del = 0, tot_conf = 0, tot_rounds = 0, max_rounds = 0;
+    long long tot_ins_eff = 0, tot_del_eff = 0, tot_recomputed_del = 0, batches_recomputed = 0;
+    double kernel_ms = 0, transfer_ms = 0;
     std::vector<int32_t> before;
     for (size_t i = 0; i < batches.size(); i++) {
         auto& b = batches[i];
@@ -218,6 +224,16 @@ int main(int argc, char** argv) {
         tot_del += st.deletions;
         tot_conf += st.conflicts;
         tot_rounds += st.rounds;
+        max_rounds = std::max<long long>(max_rounds, st.rounds);
+        tot_ins_eff += st.ins_effective;
+        if (st.variant != 0) {   // a whole-batch recompute variant settled this batch's deletions
+            batches_recomputed++;
+            tot_recomputed_del += problem == SCOUT_BFS ? st.del_effective : st.deletions - st.del_effective;
+        } else {
+            tot_del_eff += st.del_effective;
+        }
+        kernel_ms += st.ms_update + st.ms_repair;
+        transfer_ms += st.ms_h2d;
         std::vector<std::pair<std::string, std::string>> kv;
         if (problem == SCOUT_COLORING)
             kv = {{"insertions", std::to_string(st.insertions)}, {"conflicts", std::to_string(st.conflicts)},
@@ -235,13 +251,32 @@ int main(int argc, char** argv) {
     const long long final_v = measure(problem, sol);
     const char* label = problem == SCOUT_MIS ? "MIS size" : problem == SCOUT_COLORING ? "colors used"
                         : problem == SCOUT_BFS ? "reached vertices" : "components";
-    if (problem == SCOUT_BFS || problem == SCOUT_CC) {
-        std::cout << "Insertions: " << tot_ins << std::endl;
-        std::cout << "Deletions:  " << tot_del << " (deferred=0)" << std::endl;
+    // End-of-run breakdown lines (scout_bfs.cu:607-613, scout_cc.cu:531-539,
+    // scout_coloring.cu:351-357). The batch engine repairs every batch exactly, so nothing is
+    // deferred; "fallback" counts the deletions a whole-batch recompute variant settled.
+    if (problem == SCOUT_BFS) {
+        std::cout << "Insertions: " << tot_ins << " (noop=" << tot_ins - tot_ins_eff << ", repaired=" << tot_ins_eff
+                  << ")" << std::endl;
+        std::cout << "Deletions:  " << tot_del << " (noop=" << tot_del - tot_del_eff - tot_recomputed_del
+                  << ", local=" << tot_del_eff << ", fallback=" << tot_recomputed_del << ", deferred=0)" << std::endl;
+        std::cout << "  fallback (batches repaired by a full traversal): " << batches_recomputed
+                  << " | deferred catch-up: 0.000 ms | GPU kernel: " << std::fixed << std::setprecision(3) << kernel_ms
+                  << " ms | transfer: " << transfer_ms << " ms" << std::endl;
+    } else if (problem == SCOUT_CC) {
+        std::cout << "Insertions: " << tot_ins << " (noop=" << tot_ins - tot_ins_eff << ", merged=" << tot_ins_eff << ")"
+                  << std::endl;
+        std::cout << "Deletions:  " << tot_del << " (noop=0, still_connected="
+                  << tot_del - tot_del_eff - tot_recomputed_del << ", definitive_split=" << tot_del_eff
+                  << ", fallback=" << tot_recomputed_del << ", deferred=0)" << std::endl;
+        std::cout << "  fallback (batches repaired by a class recompute): " << batches_recomputed
+                  << " | deferred catch-up: 0.000 ms" << std::endl;
     } else if (problem == SCOUT_COLORING) {
-        std::cout << "Insertions: " << tot_ins << " (conflict=" << tot_conf << ")" << std::endl;
+        std::cout << "Insertions: " << tot_ins << " (noop=" << tot_ins - tot_conf << ", conflict=" << tot_conf << ")"
+                  << std::endl;
         std::cout << "Deletions:  " << tot_del << " (always a structural noop for coloring)" << std::endl;
-        std::cout << "Speculative rounds: total=" << tot_rounds << std::endl;
+        std::cout << "Speculative rounds: total=" << tot_rounds << " max_in_single_batch=" << max_rounds << std::endl;
+        std::cout << "  GPU kernel: " << std::fixed << std::setprecision(3) << kernel_ms << " ms | transfer: "
+                  << transfer_ms << " ms" << std::endl;
     }
     double compact_ms = 0;
     if (problem == SCOUT_MIS) {

@@ -287,6 +287,8 @@ static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
     st->recomputes += h.recomputes;
     st->splits = h.splits;
     st->searches = h.searches;
+    st->ins_effective = c->last_problem == SCOUT_COLORING ? h.conflicts : h.ins_eff;
+    st->del_effective = c->last_problem == SCOUT_CC ? h.splits : h.del_eff;
     st->hbm_bytes = h.hbm_bytes;
     st->update_bytes = h.update_bytes;
     st->d2h_bytes += sizeof(DevCounters);

@@ -96,13 +96,65 @@ __device__ __forceinline__ int qcount(const BfsParams& p, int qi) {
     return (long long)c > p.qcap ? (int)p.qcap : c;
 }
 
+// Work split of a round over `cnt` queue items (each at most `chunk` row entries) among the
+// grid's W warps. With at least W / 2 items, a warp takes per = ceil(cnt / W) consecutive
+// items per pass (one per lane, at most 32) and expands their entries together. With fewer
+// items, g warps share every item (g a power of two with g * cnt <= W and at least 32 entries
+// per share), each expanding its own contiguous 1/g of the item's entries: a round of a few
+// hub chunks then spreads over the whole grid instead of over a handful of warps.
+__device__ __forceinline__ int items_per_warp(int cnt, int W) {
+    const int per = (int)(((long long)cnt + W - 1) / W);
+    return per < 1 ? 1 : (per > WARP ? WARP : per);
+}
+__device__ __forceinline__ int warps_per_item(int cnt, int W, int chunk) {
+    int g = 1;
+    while ((long long)g * 2 * cnt <= W && g * 2 * WARP <= chunk) g *= 2;
+    return g;
+}
+
+// Expansion of one item share [b, e) of a row segment starting at s, 32 entries at a time;
+// every lane calls it (the pushes are warp-collective). Levels only decrease during the relax
+// rounds, so a neighbour whose level (read without an atomic, possibly stale and then larger)
+// is already at most lv + 1 needs no atomicMin.
+__device__ __forceinline__ void relax_share(const BfsParams& p, long long s, int b, int e, int lv, int nxt,
+                                            uint32_t tag) {
+    const unsigned cand = (unsigned)(lv + 1);
+    for (int k0 = b; k0 < e; k0 += WARP) {
+        const int k = k0 + (int)lane_id();
+        bool dec = false;
+        int32_t y = 0;
+        if (k < e) {
+            y = p.g.pool[s + k];
+            if ((unsigned)ld_level(p.level + y) > cand) dec = atomicMin((unsigned*)(p.level + y), cand) > cand;
+        }
+        push_vertex(p, dec, y, nxt, tag, true, true);
+    }
+}
+
 // One relax round over queue `cur` into `nxt` (warp-level load-balanced expansion).
 __device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, long long& bytes) {
     const int cnt = qcount(p, cur);
     const int W = gwarp_count();
-    for (long long gbase = (long long)gwarp_id() * WARP; gbase < cnt; gbase += (long long)W * WARP) {
+    if ((long long)cnt * 2 <= W) {
+        const int g = warps_per_item(cnt, W, p.chunk);
+        for (long long wv = gwarp_id(); wv < (long long)cnt * g; wv += W) {
+            const int item = (int)(wv / g), part = (int)(wv % g);
+            const unsigned long long it = p.q[cur][item];
+            const int32_t v = (int32_t)(it & 0xffffffffu);
+            const int chunk = (int)(it >> 32);
+            const Row r = p.g.row[v];
+            const int lv = ld_level(p.level + v);
+            const int len = lv < 0 ? 0 : max(0, min(p.chunk, r.len - (chunk << p.chunk_log2)));
+            const int b = (int)((long long)len * part / g), e = (int)((long long)len * (part + 1) / g);
+            if (lane_id() == 0) bytes += 8LL * (e - b) + (part == 0 ? 24 : 0);
+            relax_share(p, r.start + ((long long)chunk << p.chunk_log2), b, e, lv, nxt, tag);
+        }
+        return;
+    }
+    const int per = items_per_warp(cnt, W);
+    for (long long gbase = (long long)gwarp_id() * per; gbase < cnt; gbase += (long long)W * per) {
         long long idx = gbase + lane_id();
-        bool valid = idx < cnt;
+        bool valid = (int)lane_id() < per && idx < cnt;
         unsigned long long item = valid ? p.q[cur][idx] : 0ull;
         int32_t v = (int32_t)(item & 0xffffffffu);
         int chunk = (int)(item >> 32);
@@ -137,8 +189,7 @@ __device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, 
             if (e < total) {
                 y = p.g.pool[so + (e - eo)];
                 unsigned cand = (unsigned)(lo_lv + 1);
-                unsigned old = atomicMin((unsigned*)(p.level + y), cand);
-                dec = old > cand;
+                if ((unsigned)ld_level(p.level + y) > cand) dec = atomicMin((unsigned*)(p.level + y), cand) > cand;
             }
             push_vertex(p, dec, y, nxt, tag, true, true);
         }
@@ -177,13 +228,45 @@ __device__ __forceinline__ void push_new(const BfsParams& p, bool pred, int32_t 
     }
 }
 
-// Top-down step: every entry of every frontier item claims its unlevelled neighbours.
+// Top-down step: every entry of every frontier item claims its unlevelled neighbours (the
+// same work split as the relax rounds).
+__device__ __forceinline__ void td_share(const BfsParams& p, int32_t* lv, long long s, int b, int e, int d, int nxt) {
+    for (int k0 = b; k0 < e; k0 += WARP) {
+        const int k = k0 + (int)lane_id();
+        bool got = false;
+        int32_t y = 0;
+        int ylen = 0;
+        if (k < e) {
+            y = p.g.pool[s + k];
+            if (ld_volatile(lv + y) < 0) got = atomicCAS(lv + y, -1, d + 1) == -1;
+            if (got) ylen = p.g.row[y].len;
+        }
+        push_new(p, got, y, ylen, nxt);
+    }
+}
+
 __device__ void td_step(const BfsParams& p, int32_t* lv, int cur, int nxt, int d, long long& bytes) {
     const int cnt = qcount(p, cur);
     const int W = gwarp_count();
-    for (long long gbase = (long long)gwarp_id() * WARP; gbase < cnt; gbase += (long long)W * WARP) {
+    if ((long long)cnt * 2 <= W) {
+        const int g = warps_per_item(cnt, W, p.chunk);
+        for (long long wv = gwarp_id(); wv < (long long)cnt * g; wv += W) {
+            const int item = (int)(wv / g), part = (int)(wv % g);
+            const unsigned long long it = p.q[cur][item];
+            const int32_t v = (int32_t)(it & 0xffffffffu);
+            const int chunk = (int)(it >> 32);
+            const Row r = p.g.row[v];
+            const int len = max(0, min(p.chunk, r.len - (chunk << p.chunk_log2)));
+            const int b = (int)((long long)len * part / g), e = (int)((long long)len * (part + 1) / g);
+            if (lane_id() == 0) bytes += 8LL * (e - b) + (part == 0 ? 24 : 0);
+            td_share(p, lv, r.start + ((long long)chunk << p.chunk_log2), b, e, d, nxt);
+        }
+        return;
+    }
+    const int per = items_per_warp(cnt, W);
+    for (long long gbase = (long long)gwarp_id() * per; gbase < cnt; gbase += (long long)W * per) {
         long long idx = gbase + lane_id();
-        bool valid = idx < cnt;
+        bool valid = (int)lane_id() < per && idx < cnt;
         unsigned long long item = valid ? p.q[cur][idx] : 0ull;
         int32_t v = (int32_t)(item & 0xffffffffu);
         int chunk = (int)(item >> 32);
@@ -382,6 +465,8 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     cand = lx >= 0 && ly == lx + 1;
                 }
             }
+            const unsigned mc = __ballot_sync(0xffffffffu, cand);   // tree-edge deletions
+            if (lane_id() == 0 && mc) atomicAdd(&p.ctr->del_eff, __popc(mc));
             push_vertex(p, cand, y, 0, tag, true, false);
         }
         if (!grid_sync(p.bar, 2)) return;
@@ -563,6 +648,8 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
                     }
                 }
             }
+            const unsigned md = __ballot_sync(0xffffffffu, dec);   // insertions that lowered a level
+            if (lane_id() == 0 && md) atomicAdd(&p.ctr->ins_eff, __popc(md));
             push_vertex(p, dec, y, 0, tag, true, true);
         }
         if (!grid_sync(p.bar, 6)) return;

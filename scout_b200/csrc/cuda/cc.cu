@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(CC_THREADS) k_cc(CcParams p) {
         }
         if (!grid_sync(p.bar, 30)) return;
         const int nm = ld_volatile(&p.ctr->list_count[1]);
+        if (leader) p.ctr->ins_eff = nm;   // every successful hook merged two classes
         if (nm > 0) {
             for (int64_t b = tid - (tid & (WARP - 1)); b < n; b += T) {
                 int64_t v = b + lane_id();

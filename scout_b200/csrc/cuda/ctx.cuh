@@ -36,7 +36,9 @@ struct DevCounters {
     int splits;
     int searches;
     int overflow;             // a device list hit its capacity (results invalid)
-    int pad;
+    int pad;                  // CC: an edge joins two labels (inconsistent uploaded labelling)
+    int ins_eff;              // BFS: insertions that lowered a level; CC: insertions that merged classes
+    int del_eff;              // BFS: deletions of shortest-path tree edges
     long long hbm_bytes;      // algorithmic bytes of the repair
     long long aux64[4];
     unsigned long long phase_ns[8];   // %globaltimer marks written by the repair kernels

@@ -56,6 +56,13 @@ def test_bfs_cli(tmp_path):
     eng = _oracle_after("bfs", 5)
     o, a = eng.graph().csr()
     assert _final(out) == int((orc.gt_bfs(o, a, 0) >= 0).sum())
+    # end-of-run breakdown (scout_bfs.cu:607-613): the parts add up to the totals
+    ins = re.search(r"^Insertions: (\d+) \(noop=(\d+), repaired=(\d+)\)$", out, re.M)
+    dels = re.search(r"^Deletions:  (\d+) \(noop=(\d+), local=(\d+), fallback=(\d+), deferred=0\)$", out, re.M)
+    assert ins and dels, out[-600:]
+    assert int(ins.group(1)) == int(ins.group(2)) + int(ins.group(3)) == sum(int(x[2]) for x in lines)
+    assert int(dels.group(1)) == sum(int(dels.group(k)) for k in (2, 3, 4)) == sum(int(x[3]) for x in lines)
+    assert "GPU kernel:" in out
 
 
 def test_coloring_cli(tmp_path):
@@ -64,6 +71,9 @@ def test_coloring_cli(tmp_path):
     assert _final(out) == int(eng.solution().max()) + 1
     conf = [int(x) for x in re.findall(r"\| conflicts=(\d+)", out)]
     assert sum(conf) == eng.stats()["conflict"]
+    ins = re.search(r"^Insertions: (\d+) \(noop=(\d+), conflict=(\d+)\)$", out, re.M)
+    assert ins and int(ins.group(3)) == sum(conf) and int(ins.group(1)) == int(ins.group(2)) + int(ins.group(3))
+    assert re.search(r"^Speculative rounds: total=\d+ max_in_single_batch=\d+$", out, re.M)
 
 
 def test_cc_cli(tmp_path):
@@ -71,6 +81,15 @@ def test_cc_cli(tmp_path):
     eng = _oracle_after("cc", 5)
     o, a = eng.graph().csr()
     assert _final(out) == len(np.unique(orc.gt_cc(o, a)))
+    # scout_cc.cu:531-539 (the sample's batches only delete edges, none a bridge)
+    ins = re.search(r"^Insertions: (\d+) \(noop=(\d+), merged=(\d+)\)$", out, re.M)
+    dels = re.search(r"^Deletions:  (\d+) \(noop=0, still_connected=(\d+), definitive_split=(\d+), "
+                     r"fallback=(\d+), deferred=0\)$", out, re.M)
+    assert ins and dels, out[-600:]
+    assert int(ins.group(1)) == int(ins.group(2)) + int(ins.group(3))
+    assert int(ins.group(3)) == eng.stats()["merged"]
+    assert int(dels.group(1)) == sum(int(dels.group(k)) for k in (2, 3, 4))
+    assert int(dels.group(2)) == eng.stats()["still_connected"]
 
 
 def test_mis_cli_writes_set_and_compacts(tmp_path):
