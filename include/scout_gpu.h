@@ -110,6 +110,11 @@ typedef struct scout_batch_stats {
     int64_t del_effective; /* BFS: deletions of a shortest-path tree edge (the reference's
                               local + fallback); CC: deletions whose local search split
                               a component (the reference's "definitive_split")        */
+    double  ms_gather;    /* device: the gather of this batch's cold rows into HBM (tiered
+                             store, hinted by scout_prefetch; it ran on a copy stream
+                             during the previous repair), 0 when none ran             */
+    int64_t gather_rows;  /* rows that gather moved into HBM                           */
+    int64_t gather_bytes; /* bytes it read over the host link                          */
 } scout_batch_stats;
 
 typedef struct scout_ctx scout_ctx;
@@ -193,6 +198,15 @@ int scout_repair_bfs(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops
                      const scout_sched* sched, scout_batch_stats* stats);
 int scout_repair_cc(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops, int64_t m,
                     const scout_sched* sched, scout_batch_stats* stats);
+/* Hint: the edits of the batch that will follow the next scout_repair call (copied; the
+ * caller's buffer is free on return). On a tiered store, that repair call, once its own merge
+ * is done, gathers the rows of these edits' endpoints that are still in host memory into free
+ * HBM on a copy stream while its repair runs, so the hinted batch's merge and repair find
+ * them in HBM (its stats report the gather). The fetch of batch K+1 overlapping the repair of
+ * batch K replaces the reference's per-round host fetch (scout_bfs.cu:199-229) and MIS's
+ * K+1 || K channels (scout_mis.cu:855-912). On an all-HBM store it does nothing. A hint
+ * that does not match the next batch only costs the copy. */
+int scout_prefetch(scout_ctx* ctx, const scout_edge* next, int64_t m);
 /* Commit of the last repair's changed entries into a host mirror of n entries: the device
  * gathers (id, value) pairs of changed entries and copies them back; the host scatters
  * them. Replaces the gather_levels + D2H + mirror loop (scout_bfs.cu:244-262), the proposal

@@ -40,7 +40,8 @@ class ScoutBatchStats(C.Structure):
                 ("ms_repair", C.c_double), ("ms_commit", C.c_double), ("ms_total", C.c_double),
                 ("update_bytes", C.c_int64), ("launches", C.c_int64), ("ms_h2d", C.c_double),
                 ("phase_ms", C.c_double * 4), ("variant", C.c_int64), ("ms_compact", C.c_double),
-                ("compactions", C.c_int64), ("ins_effective", C.c_int64), ("del_effective", C.c_int64)]
+                ("compactions", C.c_int64), ("ins_effective", C.c_int64), ("del_effective", C.c_int64),
+                ("ms_gather", C.c_double), ("gather_rows", C.c_int64), ("gather_bytes", C.c_int64)]
 
     def as_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("reserved", "phase_ms")}
@@ -84,6 +85,7 @@ SIGNATURES = [
                                         C.POINTER(ScoutBatchStats)]),
     ("scout_repair_bfs", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
     ("scout_repair_cc", C.c_int, [_vp, _edgep, _u8p, C.c_int64, C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
+    ("scout_prefetch", C.c_int, [_vp, _edgep, C.c_int64]),
     ("scout_commit", C.c_int, [_vp, C.c_int, _i32p, C.c_int64, _i64p]),
     ("scout_recompute_bfs", C.c_int, [_vp, C.c_int32, C.POINTER(ScoutBatchStats)]),
     ("scout_recompute_cc", C.c_int, [_vp, C.POINTER(ScoutBatchStats)]),

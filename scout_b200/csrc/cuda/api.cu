@@ -59,6 +59,9 @@ int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t s
     if (per_sm < 1) return c->fail(SCOUT_E_CUDA, "persistent kernel does not fit on an SM");
     per_sm = std::min(per_sm, c->tune_blocks_per_sm > 0 ? c->tune_blocks_per_sm : 4);
     dim3 grid((unsigned)(per_sm * c->sm_count)), block((unsigned)threads);
+    // the grid barrier's arrival counter starts every launch at zero (its error flag persists
+    // until the batch's counters are read)
+    SCOUT_CU(c, cudaMemsetAsync(&c->d_bar->count, 0, sizeof(unsigned int), c->s_main));
     SCOUT_CU(c, cudaLaunchCooperativeKernel(fn, grid, block, args, smem, c->s_main));
     c->nlaunch += 1;
     return SCOUT_OK;
@@ -80,6 +83,12 @@ static void release(scout_ctx* c) {
                      c->h_slab_off[0], c->h_slab_off[1], c->h_slab_ids[0], c->h_slab_ids[1]};
     for (void* p : hosts) if (p) cudaFreeHost(p);
     for (int i = 0; i < 8; i++) if (c->ev_t[i]) cudaEventDestroy(c->ev_t[i]);
+    if (c->ev_gather0) cudaEventDestroy(c->ev_gather0);
+    if (c->ev_gather1) cudaEventDestroy(c->ev_gather1);
+    void* gdev[] = {c->gather_stamp, c->d_gctr, c->d_pf_edits, c->d_gather_list, c->d_gather_dst};
+    for (void* p : gdev) if (p) cudaFree(p);
+    if (c->h_gctr) cudaFreeHost(c->h_gctr);
+    if (c->h_pf_edits) cudaFreeHost(c->h_pf_edits);
     for (int i = 0; i < 2; i++) {
         if (c->ev_copy[i]) cudaEventDestroy(c->ev_copy[i]);
         if (c->s_copy[i]) cudaStreamDestroy(c->s_copy[i]);
@@ -174,6 +183,7 @@ int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
              cudaEventCreateWithFlags(&c->ev_copy[i], cudaEventDisableTiming) == cudaSuccess;
     }
     for (int i = 0; i < 8 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
+    ok = ok && cudaEventCreate(&c->ev_gather0) == cudaSuccess && cudaEventCreate(&c->ev_gather1) == cudaSuccess;
     ok = ok && cudaMallocHost((void**)&c->h_ctr, sizeof(DevCounters)) == cudaSuccess &&
          cudaMallocHost((void**)&c->h_bar, sizeof(GridBar)) == cudaSuccess;
     if (!ok) { cudaError_t le = cudaGetLastError(); release(c); return cuda_fail(nullptr, le, "context streams"); }
@@ -324,6 +334,9 @@ static int batch_prologue(scout_ctx* c, int problem, const scout_edge* edits, co
     if (!*slot) return c->fail(SCOUT_E_STATE, "no state uploaded for this problem");
     cudaSetDevice(c->device);
     std::memset(st, 0, sizeof(*st));
+    // the gather of this batch's cold rows, hinted by scout_prefetch and run during the previous
+    // repair, completes before the merge
+    SCOUT_RC(gather_finish(c, &st->ms_gather, &st->gather_rows, &st->gather_bytes));
     c->last_problem = problem;
     SCOUT_RC(batch_begin(c));
     SCOUT_RC(lists_ensure(c));
@@ -384,6 +397,7 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     SCOUT_RC(apply_tuning(c, sd));
     const int64_t launch0 = c->nlaunch;
     SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
+    SCOUT_RC(gather_launch(c, c->merge_tail));   // the next batch's cold rows, during this repair
     const int* mode_dev = nullptr;
     const int variant = plain_variant(problem, sd);
     if (sd.policy == SCOUT_SCHED_LEARNED && sched_variants(problem) > 1)
@@ -554,6 +568,7 @@ int scout_reserve(scout_ctx* c, int64_t max_edits) {
     if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
     cudaSetDevice(c->device);
     SCOUT_RC(graph_reserve_batch(c, max_edits));
+    SCOUT_RC(gather_reserve(c, max_edits));
     if (c->level && !c->bfs_lv) SCOUT_RC(dev_alloc(c, (void**)&c->bfs_lv, (size_t)c->n * 4, "BFS traversal levels"));
     if (c->label) SCOUT_RC(cc_ensure(c));
     if (c->color) SCOUT_RC(coloring_ensure(c));

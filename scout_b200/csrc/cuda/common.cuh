@@ -101,37 +101,46 @@ __device__ __forceinline__ bool dg_adjacent(const DGraph& g, int32_t u, int32_t 
 
 // ---------------------------------------------------------------------------------------
 // Bounded grid barrier (cooperative launch guarantees co-residency of all blocks).
+// `count` only grows within a launch: the k-th barrier is complete once it reaches k * blocks,
+// so the last block's own arrival releases the others (no reset and no second counter to bump).
+// Every block passes the same sequence of barriers, so a block arriving at barrier k sees
+// old in [(k - 1) * blocks, k * blocks). The host zeroes the block before each launch.
 // ---------------------------------------------------------------------------------------
 struct GridBar {
     unsigned int count;
-    unsigned int gen;
-    int err;          // 0 ok, 1 barrier timeout, 2 capacity overflow inside a kernel
-    int where;        // tag of the barrier that timed out
+    unsigned int gen;   // unused; kept for the layout the host reads back
+    int err;            // 0 ok, 1 barrier timeout, 2 capacity overflow inside a kernel
+    int where;          // tag of the barrier that timed out
 };
 
 constexpr uint64_t GRID_WAIT_LIMIT_NS = 4000000000ull;   // 4 s
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
 __device__ __forceinline__ bool grid_sync(GridBar* b, int tag = 0) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-        unsigned g0 = ld_volatile(&b->gen);
+        const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
         __threadfence();
-        unsigned arrived = atomicAdd(&b->count, 1u);
-        if (arrived == nb - 1) {
-            atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
-        } else {
-            uint64_t t0 = globaltimer_ns();
-            while (ld_volatile(&b->gen) == g0) {
+        const unsigned old = atomicAdd(&b->count, 1u);
+        const unsigned target = (old / nb + 1) * nb;
+        if (old + 1 != target) {
+            uint64_t t0 = 0;
+            while ((int)(ld_acquire_gpu(&b->count) - target) < 0) {
                 if (ld_volatile(&b->err)) break;
-                if (globaltimer_ns() - t0 > GRID_WAIT_LIMIT_NS) {
+                const uint64_t t = globaltimer_ns();
+                if (t0 == 0) {
+                    t0 = t;
+                } else if (t - t0 > GRID_WAIT_LIMIT_NS) {
                     if (atomicCAS(&b->err, 0, 1) == 0) b->where = tag;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         __threadfence();

@@ -87,6 +87,22 @@ struct scout_ctx {
                                     // tail, 2 split (rows from HBM to HBM, host rows to host)
     int64_t host_batches = 0;       // batches whose rows were rewritten into the host pool
     int64_t compactions = 0;
+    long long merge_tail = 0;       // HBM tail once the current batch's merge is done
+    // gather of the next batch's cold rows (tiered store; scout_prefetch, gather.cu)
+    bool pf_pending = false;        // a hint waits for the next repair's merge
+    int64_t pf_m = 0;
+    void* h_pf_edits = nullptr;  int64_t cap_h_pf_edits = 0;   // pinned copy of the hinted edits
+    scout_edge* d_pf_edits = nullptr;  int64_t cap_pf_edits = 0;
+    int32_t* gather_stamp = nullptr;   // n: last gather that took the vertex's row
+    uint32_t gather_tag = 0;
+    void* d_gctr = nullptr;
+    void* h_gctr = nullptr;            // pinned
+    int32_t* d_gather_list = nullptr;  int64_t cap_gather_list = 0;
+    long long* d_gather_dst = nullptr; int64_t cap_gather_dst = 0;
+    cudaEvent_t ev_gather0 = nullptr, ev_gather1 = nullptr;   // start / end of the gather (copy stream)
+    long long gather_base = 0;
+    bool gather_active = false;
+    int64_t gathered_rows = 0, gathered_bytes = 0;
     bool reserved = false;
     bool sealed = false;
     int32_t* d_tmp_rows = nullptr;   // staging target for rows of one slot
@@ -266,5 +282,10 @@ int sched_variants(int problem);   // repair variants a problem has (BFS 3, CC 2
 int commit_gather(scout_ctx* c, int problem, const int32_t** pairs, int64_t* count);
 // persistent launch helper
 int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem);
+// gather.cu: the hinted next batch's cold rows into free HBM from `base` on a copy stream, after
+// the current merge; gather_finish waits for it (main stream and host) and moves the tail.
+int gather_launch(scout_ctx* c, long long base);
+int gather_finish(scout_ctx* c, double* ms, int64_t* rows, int64_t* bytes);
+int gather_reserve(scout_ctx* c, int64_t max_edits);
 
 }  // namespace scout

@@ -782,6 +782,7 @@ int lists_ensure(scout_ctx* c) {
 }
 
 int batch_begin(scout_ctx* c) {
+    SCOUT_RC(gather_finish(c, nullptr, nullptr, nullptr));   // no graph work while a gather runs
     SCOUT_CU(c, cudaMemsetAsync(c->d_ctr, 0, sizeof(DevCounters), c->s_main));
     SCOUT_CU(c, cudaMemsetAsync(c->d_bar, 0, sizeof(GridBar), c->s_main));
     return SCOUT_OK;
@@ -1046,6 +1047,7 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_RC(ws_ensure(c, m));
     SCOUT_RC(graph_ensure_scratch(c));
     if (st) st->h2d_bytes += m * (int64_t)sizeof(scout_edge) + (ops ? m : 0);
+    c->merge_tail = c->tail;
     if (m == 0) {
         c->d_hkeys = c->d_keys;
         SCOUT_CU(c, cudaEventRecord(c->ev_t[3], c->s_main));
@@ -1126,6 +1128,7 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
                 return c->fail(SCOUT_E_CAPACITY, "tiered store: the host pool cannot take this batch's rows");
             SCOUT_RC(row_alloc(true, c->batch_dest == 2));
         }
+        c->merge_tail = c->tail + (c->batch_dest == 1 ? 0 : grow[0]);
         const long long host_base = elem_delta(c->host_pool, c->pool) + c->host_tail;
         if (c->batch_dest == 1) {
             dest = host_base;
@@ -1480,6 +1483,7 @@ int scout_graph_download(scout_ctx* c, int64_t* off, int32_t* adj, int64_t cap) 
     if (!c || !off) return SCOUT_E_INVALID;
     if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
     cudaSetDevice(c->device);
+    SCOUT_RC(gather_finish(c, nullptr, nullptr, nullptr));
     const int64_t n = c->n;
     int64_t* d_off = nullptr;
     SCOUT_RC(dev_alloc(c, (void**)&d_off, (size_t)(n + 1) * 8, "download offsets"));
@@ -1508,6 +1512,7 @@ int scout_graph_compact(scout_ctx* c) {
     if (!c) return SCOUT_E_INVALID;
     if (!c->sealed) return c->fail(SCOUT_E_STATE, "graph not sealed");
     cudaSetDevice(c->device);
+    SCOUT_RC(gather_finish(c, nullptr, nullptr, nullptr));
     return graph_compact(c, std::max<int64_t>(c->nnz, 1 << 22), true);
 }
 

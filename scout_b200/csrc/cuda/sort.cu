@@ -315,10 +315,47 @@ __global__ void k_scan_apply(T* __restrict__ a, int64_t n, const int64_t* __rest
     }
 }
 
+// Arrays of up to SCAN_ONE_MAX entries are scanned by one 1024-thread block in one launch (each
+// thread a contiguous run of at most 64 entries); longer ones by the three-launch tile scan.
+constexpr int64_t SCAN_ONE_MAX = 1 << 16;
+constexpr int SCAN_ONE_THREADS = 1024;
+
+template <typename T>
+__global__ void __launch_bounds__(SCAN_ONE_THREADS) k_scan_one(T* __restrict__ a, int64_t n, int64_t* __restrict__ d_total) {
+    __shared__ long long ws[SCAN_ONE_THREADS / WARP];
+    const int t = threadIdx.x, w = t / WARP, lane = t & (WARP - 1);
+    const int64_t per = (n + SCAN_ONE_THREADS - 1) / SCAN_ONE_THREADS;
+    const int64_t lo = (int64_t)t * per, hi = lo + per < n ? lo + per : n;
+    long long s = 0;
+    for (int64_t i = lo; i < hi; i++) s += (long long)a[i];
+    const long long inc = warp_incl_scan(s);
+    if (lane == WARP - 1) ws[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const long long v = ws[lane];
+        const long long vi = warp_incl_scan(v);
+        ws[lane] = vi - v;
+        if (lane == WARP - 1 && d_total) *d_total = vi;
+    }
+    __syncthreads();
+    long long run = ws[w] + inc - s;
+    for (int64_t i = lo; i < hi; i++) {
+        const long long x = (long long)a[i];
+        a[i] = (T)run;
+        run += x;
+    }
+}
+
 template <typename T>
 static int scan_any(scout_ctx* c, T* data, int64_t n, int64_t* d_total) {
     if (n <= 0) {
         if (d_total) SCOUT_CU(c, cudaMemsetAsync(d_total, 0, sizeof(int64_t), c->s_main));
+        return SCOUT_OK;
+    }
+    if (n <= SCAN_ONE_MAX) {
+        k_scan_one<T><<<1, SCAN_ONE_THREADS, 0, c->s_main>>>(data, n, d_total);
+        SCOUT_LAUNCH(c, "k_scan_one");
+        c->nlaunch += 1;
         return SCOUT_OK;
     }
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;

@@ -219,6 +219,12 @@ class Context:
         self._c(LIB.scout_repair(self._h, _prob(problem), _pedge(e), op, len(e), C.byref(sd), C.byref(st)))
         return st.as_dict()
 
+    def prefetch(self, next_edges) -> None:
+        """Hint the edits of the batch after the next repair (tiered store: its cold rows are
+        gathered into HBM while that repair runs)."""
+        e = as_edges(next_edges)
+        self._c(LIB.scout_prefetch(self._h, _pedge(e), len(e)))
+
     def repair_probe(self, problem, edges, ops=None, sched: Optional[dict] = None):
         """One batch, every repair variant timed from the same pre-repair state (results must
         agree). Returns (stats, variant_ms[3] with -1 for absent variants, features[24])."""
