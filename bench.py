@@ -476,12 +476,34 @@ def scout_arm(a, dist):
 # ---------------------------------------------------------------------------------------
 # out-of-core section: a graph 4.3x larger than its HBM pool (the 16 GB / 69 GB ratio)
 # ---------------------------------------------------------------------------------------
+def h2d_peak_gbs(device: int, mib: int = 1024, reps: int = 5) -> float:
+    """Host-to-device copy bandwidth from page-locked memory (the host link's measured peak):
+    the best of `reps` copies of `mib` MiB, timed with CUDA events."""
+    import torch
+    src = torch.empty(mib << 20, dtype=torch.uint8).pin_memory()
+    dst = torch.empty(mib << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    best = 0.0
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize(device)
+        best = max(best, (mib << 20) / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del src, dst
+    return best
+
+
 def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
     """BFS and CC streams of deletion-heavy batches (70% deletions of existing edges, 30% of
     them with a low-degree first endpoint; 30% uniform insertions) on an R-MAT graph of scale
     a.ooc_scale, edge factor 32, whose HBM element pool holds 23% of the adjacency: hot rows
-    in HBM, the rest in mapped page-locked host memory read in place. Plain and learned
-    scheduling on the tiered store, and the all-in-HBM engine on the same stream for scale."""
+    in HBM, the rest in mapped page-locked host memory. Arms on the tiered store: plain (cold
+    rows read in place, plain scheduling), learned (the cost model picks the variant),
+    batched (each batch's cold endpoint rows gathered into HBM on a copy stream during the
+    previous batch's repair, scout_prefetch) and learned + batched; the all-in-HBM engine on the
+    same stream for scale. The gather's bytes over its time, against the measured host-link
+    peak, is the host-link roofline."""
     import scout_b200 as sb
     g = sb.gen_rmat(a.ooc_scale, 32, seed=29)
     off, adj = g.arrays()
@@ -489,17 +511,20 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
     hbm = int(0.23 * nnz)
     s = g.stream(sb.STREAM_LOWDEG, m, nbatches, insert_ratio=0.3, lowdeg_frac=0.3, seed=2929)
     batches = [sb.pinned_copy(x) for x in s.reshape(nbatches, m, 2)]
+    peak = h2d_peak_gbs(device)
     out = {"workload": f"R-MAT scale {a.ooc_scale} EF32 seed 29 ({g.n} vertices, {nnz} directed entries, "
                        f"{4 * nnz / 1e9:.2f} GB adjacency); HBM pool {hbm} entries (23%); {nbatches} batches of "
                        f"{m} toggles: 70% deletions (30% low-degree first endpoint), 30% uniform insertions",
-           "vertices": int(g.n), "directed_entries": nnz}
+           "vertices": int(g.n), "directed_entries": nnz, "h2d_peak_gbs": peak,
+           "h2d_peak": "best of 5 copies of 1 GiB from page-locked host memory, CUDA events"}
     for p in ("bfs", "cc"):
         init = g.init_state(p, 0)
         res = {}
-        arms = [("tiered_plain", True, None), ("in_hbm_plain", False, None)]
+        arms = [("tiered_plain", True, None, False), ("tiered_batched", True, None, True)]
         if p in model:
-            arms.insert(1, ("tiered_learned", True, model[p]))
-        for arm, tier, mdl in arms:
+            arms += [("tiered_learned", True, model[p], False), ("tiered_learned_batched", True, model[p], True)]
+        arms.append(("in_hbm_plain", False, None, False))
+        for arm, tier, mdl, batched in arms:
             with sb.Context(device) as ctx:
                 if tier:
                     ctx.load_tiered(off, adj, hbm_entries=hbm)
@@ -514,8 +539,12 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
                 mirror = init.copy()
                 dev = wall = 0.0
                 lat, variants = [], []
-                for b in batches:
+                g_bytes = g_ms = 0.0
+                g_rows = 0
+                for k, b in enumerate(batches):
                     t0 = time.perf_counter()
+                    if batched and k + 1 < len(batches):
+                        ctx.prefetch(batches[k + 1])
                     st = ctx.repair(p, b, sched=sched)
                     ctx.commit(p, mirror)
                     dt = 1e3 * (time.perf_counter() - t0)
@@ -523,15 +552,25 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
                     lat.append(dt)
                     dev += st["ms_compact"] + st["ms_update"] + st["ms_repair"]
                     variants.append(int(st["variant"]))
+                    g_bytes += st["gather_bytes"]
+                    g_ms += st["ms_gather"]
+                    g_rows += st["gather_rows"]
                     if a.verbose:
                         print(f"out_of_core {p} {arm}: wall {dt:.1f} ms, update {st['ms_update']:.1f}, repair "
-                              f"{st['ms_repair']:.1f}, compact {st['ms_compact']:.1f}, variant {st['variant']}, "
-                              f"tiers {ctx.tier_info()}", file=sys.stderr, flush=True)
+                              f"{st['ms_repair']:.1f}, compact {st['ms_compact']:.1f}, gather {st['ms_gather']:.1f} ms "
+                              f"({st['gather_rows']} rows), variant {st['variant']}, tiers {ctx.tier_info()}",
+                              file=sys.stderr, flush=True)
                 info = ctx.tier_info()
             edits = nbatches * m
-            res[arm] = {"edge_updates_per_s": edits / (dev / 1e3), "e2e_edge_updates_per_s": edits / (wall / 1e3),
-                        "p99_batch_ms": float(np.percentile(lat, 99)), "variants": variants,
-                        "hbm_used": info["hbm_used"], "host_used": info["host_used"], "evicted": info["evicted"]}
+            r = {"edge_updates_per_s": edits / (dev / 1e3), "e2e_edge_updates_per_s": edits / (wall / 1e3),
+                 "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
+                 "variants": variants, "hbm_used": info["hbm_used"], "host_used": info["host_used"],
+                 "evicted": info["evicted"]}
+            if batched:
+                gbs = g_bytes / (g_ms / 1e3) / 1e9 if g_ms else 0.0
+                r["gather"] = {"rows": g_rows, "bytes": g_bytes, "ms": g_ms, "achieved_gbs": gbs,
+                               "frac_of_h2d_peak": gbs / peak if peak else None}
+            res[arm] = r
         base = res["tiered_plain"]["e2e_edge_updates_per_s"]
         for r in res.values():
             r["e2e_vs_tiered_plain"] = r["e2e_edge_updates_per_s"] / base

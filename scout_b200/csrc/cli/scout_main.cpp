@@ -207,6 +207,11 @@ int main(int argc, char** argv) {
         auto& b = batches[i];
         scout_batch_stats st;
         auto t0 = clk::now();
+        // the next batch's cold rows (a graph beyond the device budget) are gathered during this
+        // repair, as the reference's MIS pipeline prepares batch K+1 while K runs
+        // (scout_mis.cu:855-912); a graph held wholly in HBM ignores the hint
+        if (i + 1 < batches.size() && !batches[i + 1].empty())
+            scout_prefetch(ctx, batches[i + 1].data(), (int64_t)batches[i + 1].size());
         int rc = scout_repair(ctx, problem, b.data(), ops[i].empty() ? nullptr : ops[i].data(), (int64_t)b.size(),
                               nullptr, &st);
         if (rc != SCOUT_OK) die("repair failed", scout_last_error(ctx));
