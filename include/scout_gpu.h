@@ -61,9 +61,13 @@ enum scout_frontier { SCOUT_FRONTIER_AUTO = 0, SCOUT_FRONTIER_QUEUE = 1, SCOUT_F
 typedef struct scout_sched {
     int32_t policy;           /* scout_policy                                       */
     int32_t mode;             /* scout_mode: incremental repair vs full recompute    */
-    int32_t frontier;         /* scout_frontier                                     */
-    int32_t lanes_per_vertex; /* ignored: every kernel scans rows a warp at a time and
-                                 splits long rows into chunk_log2-sized items instead    */
+    int32_t frontier;         /* scout_frontier: with mode RECOMPUTE, the BFS traversal's
+                                 frontier (QUEUE: top-down queue; BITMAP or AUTO:
+                                 direction-optimizing, bottom-up steps over the level array) */
+    int32_t lanes_per_vertex; /* BFS expansion: most lanes that share one queue item (one
+                                 chunk_log2-sized slice of a row) when a round has fewer
+                                 items than warps: 32, 64, 128, 256 or 1024 (1-32 warps);
+                                 0 = as many warps as the item and the grid allow        */
     int64_t search_bound;     /* CC local-search bound (vertices); 0 = reference rule */
     int64_t search_limit;     /* CC: a class with more deletions left to search than this is
                                  recomputed instead (0 = 32; < 0 = always search)        */

@@ -1,19 +1,25 @@
 """Autotuner of the engine's launch knobs.
 
-Knobs (all exact: they change speed, never results):
-  blocks_per_sm   resident blocks per SM of the persistent repair kernels (1, 2, 4): more
-                  blocks hide latency, fewer make each grid barrier cheaper
-  chunk_log2      BFS queue item = 2^chunk_log2 row entries (8 .. 13): smaller items spread a
-                  hub's row over more warps, larger ones cost fewer queue entries
-  round_cap       multi-stream engine: most edits per round (2^16 .. 2^22): larger rounds
-                  amortise the per-round fixed cost over more streams, smaller ones bound the
-                  latency a small batch waits behind large ones
-The repair variant (incremental, top-down queue traversal, direction-optimizing bitmap
-traversal) is chosen per batch by the scheduler, not here.
+Knobs (all exact: they change speed, never results; every configuration's final solution is
+checksummed and the sweep fails if two differ):
+  blocks_per_sm     resident blocks per SM of the persistent repair kernels (1, 2, 4): more
+                    blocks hide latency, fewer make each grid barrier cheaper
+  chunk_log2        BFS queue item = 2^chunk_log2 row entries (8 .. 13): smaller items spread a
+                    hub's row over more warps, larger ones cost fewer queue entries
+  lanes_per_vertex  BFS: most lanes sharing one queue item when a round has fewer items than
+                    warps (32, 64, 128, 256, 1024, i.e. 1-32 warps; 0 = as many as useful)
+  mode / frontier   the plain engine's repair variant: incremental, or a full traversal with a
+                    queue frontier (top-down) or a bitmap frontier (direction-optimizing); CC:
+                    incremental or a recompute of every class. The learned scheduler picks the
+                    variant per batch instead
+  round_cap         multi-stream engine: most edits per round (2^16 .. 2^22): larger rounds
+                    amortise the per-round fixed cost over more streams, smaller ones bound the
+                    latency a small batch waits behind large ones
 
 Each configuration replays the same sample batches from the same starting state on a fresh
 context and is scored by the library's device time (CUDA events on its stream) over the
-sample, after one warm-up batch.
+sample, after one warm-up batch. The defaults (blocks 4, chunk 10, lanes 0, incremental) are
+always among the configurations, so the choice is never slower than them on the sample.
 
     python -m scout_b200.autotune --out scout_b200/tuned.json
 """
@@ -31,33 +37,72 @@ from ._lib import STREAM_PREFERENTIAL
 
 BLOCKS = (1, 2, 4)
 CHUNKS = (8, 10, 12)
+LANES = (0, 32, 64, 128, 256, 1024)
 CAPS = (1 << 16, 1 << 18, 1 << 20, 1 << 22)
+DEFAULT = {"blocks_per_sm": 4, "chunk_log2": 10, "lanes_per_vertex": 0, "mode": 0, "frontier": 0}
+# plain repair variants: (mode, frontier); SCOUT_MODE_RECOMPUTE = 2, QUEUE = 1, BITMAP = 2
+VARIANTS = {"bfs": ((0, 0), (2, 1), (2, 2)), "cc": ((0, 0), (2, 0))}
 
 
 def _device_ms(st: dict) -> float:
     return st["ms_compact"] + st["ms_update"] + st["ms_repair"]
 
 
-def tune_single(problem, off, adj, init, batches, device: int = 0, blocks=BLOCKS, chunks=CHUNKS, model=None) -> dict:
-    """Sweeps blocks_per_sm x chunk_log2 (chunk only matters for BFS) on one stream."""
+def run_config(problem, off, adj, init, batches, sched: dict, device: int = 0, model=None):
+    """(device ms over batches[1:], crc32 of the final solution) of one configuration."""
+    import zlib
+    sd = dict(sched)
+    if model is not None:
+        sd["policy"] = 1
+    with E.Context(device) as ctx:
+        ctx.load_csr(off, adj)
+        ctx.upload(problem, init)
+        if model is not None:
+            ctx.sched_install(problem, model)
+        ctx.reserve_batches(max(len(b) for b in batches))
+        ctx.repair(problem, batches[0], sched=sd)
+        ms = sum(_device_ms(ctx.repair(problem, b, sched=sd)) for b in batches[1:])
+        crc = zlib.crc32(np.ascontiguousarray(ctx.download(problem)).tobytes())
+    return ms, crc
+
+
+def tune_single(problem, off, adj, init, batches, device: int = 0, blocks=BLOCKS, chunks=CHUNKS, lanes=LANES,
+                model=None, variants: bool = True) -> dict:
+    """Sweeps blocks_per_sm x chunk_log2 (chunk only matters for BFS), then at the best of
+    those lanes_per_vertex (BFS) and the plain repair variant (BFS, CC) on one stream."""
     chunks = chunks if problem == "bfs" else (10,)
     table = []
+
+    def run(cfg):
+        ms, crc = run_config(problem, off, adj, init, batches, cfg, device, model)
+        row = dict(cfg, device_ms=ms, solution_crc=crc)
+        table.append(row)
+        return row
+
+    run(dict(DEFAULT))
     for bps, ch in itertools.product(blocks, chunks):
-        sched = {"blocks_per_sm": bps, "chunk_log2": ch}
-        if model is not None:
-            sched["policy"] = 1
-        with E.Context(device) as ctx:
-            ctx.load_csr(off, adj)
-            ctx.upload(problem, init)
-            if model is not None:
-                ctx.sched_install(problem, model)
-            ctx.reserve_batches(max(len(b) for b in batches))
-            ctx.repair(problem, batches[0], sched=sched)
-            ms = sum(_device_ms(ctx.repair(problem, b, sched=sched)) for b in batches[1:])
-        table.append({"blocks_per_sm": bps, "chunk_log2": ch, "device_ms": ms})
-    best = min(table, key=lambda r: r["device_ms"])
-    return {"problem": problem, "best": {"blocks_per_sm": best["blocks_per_sm"], "chunk_log2": best["chunk_log2"]},
-            "table": table}
+        cfg = dict(DEFAULT, blocks_per_sm=bps, chunk_log2=ch)
+        if cfg != DEFAULT:
+            run(cfg)
+    best = dict(min(table, key=lambda r: r["device_ms"]))
+    if problem == "bfs":
+        base = {k: best[k] for k in DEFAULT}
+        for lv in lanes:
+            cfg = dict(base, lanes_per_vertex=lv)
+            if cfg != base:
+                run(cfg)
+        best = dict(min(table, key=lambda r: r["device_ms"]))
+    if variants and problem in VARIANTS and model is None:
+        base = {k: best[k] for k in DEFAULT}
+        for mode, fr in VARIANTS[problem]:
+            cfg = dict(base, mode=mode, frontier=fr)
+            if cfg != base:
+                run(cfg)
+        best = dict(min(table, key=lambda r: r["device_ms"]))
+    crcs = {r["solution_crc"] for r in table}
+    if len(crcs) != 1:
+        raise RuntimeError(f"{problem}: launch knobs changed the solution ({len(crcs)} different results)")
+    return {"problem": problem, "best": {k: best[k] for k in DEFAULT}, "table": table}
 
 
 def tune_rounds(problem, streams, arrivals, device: int = 0, caps=CAPS, sched=None) -> dict:

@@ -321,8 +321,14 @@ static int apply_tuning(scout_ctx* c, const scout_sched& sd) {
     if (sd.blocks_per_sm < 0 || sd.blocks_per_sm > 4) return c->fail(SCOUT_E_INVALID, "blocks_per_sm must be 0..4");
     if (sd.chunk_log2 != 0 && (sd.chunk_log2 < 8 || sd.chunk_log2 > 13))
         return c->fail(SCOUT_E_INVALID, "chunk_log2 must be 0 or 8..13");
+    const int lpv = sd.lanes_per_vertex;
+    if (!(lpv == 0 || lpv == 32 || lpv == 64 || lpv == 128 || lpv == 256 || lpv == 1024))
+        return c->fail(SCOUT_E_INVALID, "lanes_per_vertex must be 0, 32, 64, 128, 256 or 1024");
+    if (sd.frontier < SCOUT_FRONTIER_AUTO || sd.frontier > SCOUT_FRONTIER_BITMAP)
+        return c->fail(SCOUT_E_INVALID, "unknown frontier mode");
     c->tune_blocks_per_sm = sd.blocks_per_sm;
     c->tune_chunk_log2 = sd.chunk_log2 ? sd.chunk_log2 : 10;
+    c->tune_share = lpv / 32;
     return SCOUT_OK;
 }
 

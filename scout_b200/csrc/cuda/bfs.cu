@@ -51,6 +51,7 @@ struct BfsParams {
     int chunk, chunk_log2;    // row entries per queue item (a power of two, 256 .. 8192)
     const int32_t* sources;   // when nsrc > 0: every listed vertex is a level-0 root (a union of
     int nsrc;                 // disjoint graphs, one source each); else `source` alone
+    int max_share;            // most warps that share one queue item (lanes_per_vertex / 32)
 };
 
 __device__ __forceinline__ int32_t ld_level(const int32_t* p) { return ld_volatile(p); }
@@ -106,9 +107,9 @@ __device__ __forceinline__ int items_per_warp(int cnt, int W) {
     const int per = (int)(((long long)cnt + W - 1) / W);
     return per < 1 ? 1 : (per > WARP ? WARP : per);
 }
-__device__ __forceinline__ int warps_per_item(int cnt, int W, int chunk) {
+__device__ __forceinline__ int warps_per_item(int cnt, int W, int chunk, int max_share) {
     int g = 1;
-    while ((long long)g * 2 * cnt <= W && g * 2 * WARP <= chunk) g *= 2;
+    while ((long long)g * 2 * cnt <= W && g * 2 * WARP <= chunk && g * 2 <= max_share) g *= 2;
     return g;
 }
 
@@ -136,7 +137,7 @@ __device__ void relax_round(const BfsParams& p, int cur, int nxt, uint32_t tag, 
     const int cnt = qcount(p, cur);
     const int W = gwarp_count();
     if ((long long)cnt * 2 <= W) {
-        const int g = warps_per_item(cnt, W, p.chunk);
+        const int g = warps_per_item(cnt, W, p.chunk, p.max_share);
         for (long long wv = gwarp_id(); wv < (long long)cnt * g; wv += W) {
             const int item = (int)(wv / g), part = (int)(wv % g);
             const unsigned long long it = p.q[cur][item];
@@ -249,7 +250,7 @@ __device__ void td_step(const BfsParams& p, int32_t* lv, int cur, int nxt, int d
     const int cnt = qcount(p, cur);
     const int W = gwarp_count();
     if ((long long)cnt * 2 <= W) {
-        const int g = warps_per_item(cnt, W, p.chunk);
+        const int g = warps_per_item(cnt, W, p.chunk, p.max_share);
         for (long long wv = gwarp_id(); wv < (long long)cnt * g; wv += W) {
             const int item = (int)(wv / g), part = (int)(wv % g);
             const unsigned long long it = p.q[cur][item];
@@ -708,6 +709,7 @@ static int bfs_launch(scout_ctx* c, int mode, const int* mode_dev, scout_batch_s
     p.sources = c->d_sources;
     p.nsrc = c->nsrc;
     p.chunk_log2 = c->tune_chunk_log2;
+    p.max_share = c->tune_share > 0 ? c->tune_share : (1 << 20);
     p.chunk = 1 << p.chunk_log2;
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_bfs, BFS_THREADS, args, 0);

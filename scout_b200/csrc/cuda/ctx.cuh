@@ -47,7 +47,8 @@ struct DevCounters {
     int sched_del_hit;        // deletion half-edits meeting the problem's structural test
     int sched_del;            // deletion half-edits
     int decision;             // repair variant the kernels run (read on the device)
-    int sort_err;             // 1: a sort look-back wait timed out, 2: a sort position out of range
+    int sort_err;             // 1: a sort look-back wait timed out, 2: a sort position out of range,
+                              // 3: a bulk copy into shared memory (row merge) did not complete
     int sched_flags;          // 1 features computed, 2 model applied
     float feat[24];
     float pred[4];
@@ -191,6 +192,7 @@ struct scout_ctx {
     // tuning knobs of the current call (scout_sched.blocks_per_sm / chunk_log2)
     int tune_blocks_per_sm = 0;   // 0: as many as fit, at most 4
     int tune_chunk_log2 = 10;     // BFS queue item = 2^chunk_log2 row entries
+    int tune_share = 0;           // most warps sharing one BFS queue item (0: as many as useful)
     int64_t nlaunch = 0;       // kernels launched (running count)
 
     int fail(int code, const std::string& msg) { err = msg; return code; }

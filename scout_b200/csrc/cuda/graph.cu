@@ -472,16 +472,109 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
 // Long rows: one warp per slice of SLICE old-row entries. The survivors before the slice are
 // its start minus the matched deletions before it (one search in the non-decreasing dpos);
 // survivor x lands at (#survivors before it) + (#insertions < x), the insertion count
-// searched only inside the range spanned by the chunk's values. Four coalesced loads per
-// lane per chunk.
-__global__ void k_merge_slices(int32_t* __restrict__ pool, const unsigned long long* __restrict__ keys, int B,
-                               const DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg,
-                               const Row* __restrict__ old_row, const int64_t* __restrict__ off, long long tail,
-                               const long long* __restrict__ E, const long long* __restrict__ dpos,
-                               const int64_t* __restrict__ slices, int64_t slice_cap) {
+// searched only inside the range spanned by the chunk's values.
+//
+// A slice of an HBM row is staged in shared memory by the bulk-copy engine: each warp owns two
+// MS_CH-entry buffers and their mbarriers; lane 0 issues cp.async.bulk (non-multicast) of the
+// 16-byte-aligned cover of the next chunk while the warp merges the current one from shared
+// memory, so the old row is read in MS_CH * 4-byte transfers with no load instruction per
+// entry. Every wait on an mbarrier is bounded: past the limit the warp flags sort_err = 3,
+// waits (bounded again) for its copies in flight and leaves. Rows in host memory (tiered
+// store) and slices whose aligned cover would pass the pool's end are read with direct loads.
+constexpr int MS_WARPS = 8;
+constexpr int MS_THREADS = MS_WARPS * WARP;
+constexpr int MS_CH = 512;                 // entries per staged chunk
+constexpr int MS_BUF = MS_CH + 8;          // buffer: chunk + 16-byte alignment slack on both ends
+constexpr long long MBAR_SPIN_LIMIT = 1ll << 24;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// lane 0: one arrival that expects `bytes`, then the bulk copy global -> shared completing on bar
+__device__ __forceinline__ void bulk_g2s(int32_t* dst, const int32_t* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// all lanes: bounded wait for the given phase of bar; false when the limit was reached
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (long long it = 0; it < MBAR_SPIN_LIMIT; it++) {
+        if (mbar_test(bar, parity)) return true;
+        if (it > 64) __nanosleep(128);
+    }
+    return false;
+}
+
+// Merges old-row entries [b, e) (absolute pool indices) read through `get`, updating the running
+// survivor count; every lane calls it.
+template <typename Get>
+__device__ __forceinline__ void merge_span(long long b, long long e, Get get, int32_t* out, long long& run,
+                                           const KeySpan& I, long long p, unsigned lt) {
     constexpr int U = 4;
-    const long long nsl = min((long long)ctr->n_slices, (long long)slice_cap);
+    for (long long base = b; base < e; base += U * WARP) {
+        int32_t x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const long long i = base + u * WARP + lane_id();
+            x[u] = i < e ? get(i) : -1;
+        }
+        long long cl = 0, ch = 0;
+        if (p > 0) {
+            int xmin = INT32_MAX, xmax = -1;
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (x[u] >= 0) { xmin = min(xmin, x[u]); xmax = max(xmax, x[u]); }
+            xmin = __reduce_min_sync(0xffffffffu, xmin);
+            xmax = __reduce_max_sync(0xffffffffu, xmax);
+            if (xmax >= 0 && lane_id() == 0) {
+                cl = lb_span(I, p, xmin);
+                ch = cl + lb_span(KeySpan{I.k + cl, I.B}, p - cl, xmax);
+            }
+            cl = __shfl_sync(0xffffffffu, cl, 0);
+            ch = __shfl_sync(0xffffffffu, ch, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool surv = x[u] >= 0;
+            const unsigned m = __ballot_sync(0xffffffffu, surv);
+            if (surv) {
+                long long lbI = cl;
+                if (ch > cl) lbI = cl + lb_span(KeySpan{I.k + cl, I.B}, ch - cl, x[u]);
+                out[run + __popc(m & lt) + lbI] = x[u];
+            }
+            run += __popc(m);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
+        int32_t* __restrict__ pool, long long pool_cap, const unsigned long long* __restrict__ keys, int B,
+        DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
+        const int64_t* __restrict__ off, long long tail, const long long* __restrict__ E,
+        const long long* __restrict__ dpos, const int64_t* __restrict__ slices, int64_t slice_cap) {
+    __shared__ __align__(16) int32_t s_buf[MS_WARPS][2][MS_BUF];
+    __shared__ __align__(8) uint64_t s_bar[MS_WARPS][2];
+    const int w = threadIdx.x / WARP;
     const unsigned lt = (1u << lane_id()) - 1;
+    if (lane_id() == 0) {
+        mbar_init(&s_bar[w][0]);
+        mbar_init(&s_bar[w][1]);
+        fence_proxy_async_smem();   // the initialised barriers are visible to the bulk-copy engine
+    }
+    __syncwarp();
+    unsigned phase[2] = {0u, 0u};
+    const long long nsl = min((long long)ctr->n_slices, (long long)slice_cap);
     for (long long it = gwarp_id(); it < nsl; it += gwarp_count()) {
         const long long item = slices[it];
         const int a = (int)(item >> 32), s = (int)(item & 0xffffffffLL);
@@ -497,41 +590,41 @@ __global__ void k_merge_slices(int32_t* __restrict__ pool, const unsigned long l
             md = E[sp + lo] - E[sp];
         }
         long long run = s0 - __shfl_sync(0xffffffffu, md, 0);
-        const int32_t* O = pool + r.start;
         int32_t* out = pool + tail + off[a];
-        KeySpan I{keys + b0, B};
-        for (long long base = s0; base < s1; base += U * WARP) {
-            int32_t x[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const long long i = base + u * WARP + lane_id();
-                x[u] = i < s1 ? O[i] : -1;
+        const KeySpan I{keys + b0, B};
+        const long long abs0 = r.start + s0, abs1 = r.start + s1;   // pool indices of the slice
+        const bool staged = r.start >= 0 && ((abs1 + 3) & ~3LL) <= pool_cap;
+        if (!staged) {
+            merge_span(abs0, abs1, [&](long long i) { return pool[i]; }, out, run, I, p, lt);
+            continue;
+        }
+        const int nch = (int)((s1 - s0 + MS_CH - 1) / MS_CH);
+        auto issue = [&](int k) {   // lane 0
+            const long long lo = abs0 + (long long)k * MS_CH, hi = min(abs1, lo + MS_CH);
+            const long long a0 = lo & ~3LL, a1 = (hi + 3) & ~3LL;
+            bulk_g2s(s_buf[w][k & 1], pool + a0, (unsigned)((a1 - a0) * 4), &s_bar[w][k & 1]);
+        };
+        if (lane_id() == 0) {
+            issue(0);
+            if (nch > 1) issue(1);
+        }
+        for (int k = 0; k < nch; k++) {
+            const int bsel = k & 1;
+            if (!mbar_wait(&s_bar[w][bsel], phase[bsel])) {
+                // give up: flag it, let the copies in flight land (bounded), leave
+                if (lane_id() == 0) atomicCAS(&ctr->sort_err, 0, 3);
+                mbar_wait(&s_bar[w][bsel], phase[bsel]);
+                if (k + 1 < nch) mbar_wait(&s_bar[w][bsel ^ 1], phase[bsel ^ 1]);
+                return;
             }
-            long long cl = 0, ch = 0;
-            if (p > 0) {
-                int xmin = INT32_MAX, xmax = -1;
-#pragma unroll
-                for (int u = 0; u < U; u++)
-                    if (x[u] >= 0) { xmin = min(xmin, x[u]); xmax = max(xmax, x[u]); }
-                xmin = __reduce_min_sync(0xffffffffu, xmin);
-                xmax = __reduce_max_sync(0xffffffffu, xmax);
-                if (xmax >= 0 && lane_id() == 0) {
-                    cl = lb_span(I, p, xmin);
-                    ch = cl + lb_span(KeySpan{I.k + cl, B}, p - cl, xmax);
-                }
-                cl = __shfl_sync(0xffffffffu, cl, 0);
-                ch = __shfl_sync(0xffffffffu, ch, 0);
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool surv = x[u] >= 0;
-                const unsigned m = __ballot_sync(0xffffffffu, surv);
-                if (surv) {
-                    long long lbI = cl;
-                    if (ch > cl) lbI = cl + lb_span(KeySpan{I.k + cl, B}, ch - cl, x[u]);
-                    out[run + __popc(m & lt) + lbI] = x[u];
-                }
-                run += __popc(m);
+            phase[bsel] ^= 1u;
+            const long long lo = abs0 + (long long)k * MS_CH, hi = min(abs1, lo + MS_CH);
+            const int32_t* sb = s_buf[w][bsel] - (lo & ~3LL);   // indexed by absolute pool index
+            merge_span(lo, hi, [&](long long i) { return sb[i]; }, out, run, I, p, lt);
+            __syncwarp();   // every lane is done with this buffer before it is refilled
+            if (k + 2 < nch && lane_id() == 0) {
+                fence_proxy_async_smem();   // the warp's reads of the buffer precede the copy's writes
+                issue(k + 2);
             }
         }
     }
@@ -798,6 +891,7 @@ int counters_fetch(scout_ctx* c) {
         return c->fail(SCOUT_E_STATE, "the component labels do not describe the components of the graph "
                                       "(an edge joins two labels); upload a consistent labelling");
     if (c->h_ctr->sort_err == 1) return c->fail(SCOUT_E_TIMEOUT, "a sort look-back wait timed out");
+    if (c->h_ctr->sort_err == 3) return c->fail(SCOUT_E_TIMEOUT, "a bulk copy of a row slice into shared memory did not complete");
     if (c->h_ctr->sort_err) return c->fail(SCOUT_E_STATE, "the sort computed a position out of range");
     if (c->h_bar->err != 0 || c->h_ctr->overflow)
         return c->fail(SCOUT_E_CAPACITY, "a device work list overflowed its capacity");
@@ -1157,9 +1251,9 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     k_merge_small<<<blocks_for(groups * WARP, MERGE_THREADS), MERGE_THREADS, 0, c->s_main>>>(
         c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, dest, c->d_aff_small,
         c->d_small_off);
-    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, 256), 256, 0,
-                     c->s_main>>>(c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len,
-                                  dest, E, dpos, c->d_slices, c->cap_slices);
+    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, MS_THREADS), MS_THREADS,
+                     0, c->s_main>>>(c->pool, (long long)c->pool_cap, sorted, B, c->d_ctr, c->d_aff_seg,
+                                     c->d_old_row, c->d_aff_len, dest, E, dpos, c->d_slices, c->cap_slices);
     SCOUT_LAUNCH(c, "merge");
     c->nlaunch += 5;
     return SCOUT_OK;
