@@ -62,9 +62,9 @@ def parse_args():
     ap.add_argument("--no-multi", action="store_true", help="skip the multi-stream section")
     ap.add_argument("--multi-batches", type=int, default=6, help="batches per stream in the multi-stream section")
     ap.add_argument("--no-ooc", action="store_true", help="skip the out-of-core section")
-    ap.add_argument("--ooc-scale", type=int, default=21)
-    ap.add_argument("--ooc-batches", type=int, default=4)
-    ap.add_argument("--ooc-edits", type=int, default=250_000)
+    ap.add_argument("--ooc-scale", type=int, default=23)
+    ap.add_argument("--ooc-batches", type=int, default=5)
+    ap.add_argument("--ooc-edits", type=int, default=100_000)
     return ap.parse_args()
 
 

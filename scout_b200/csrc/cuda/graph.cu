@@ -1205,8 +1205,19 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
             return SCOUT_OK;
         };
         SCOUT_RC(read_grow());
-        if (c->tail + grow[0] + 1024 > c->pool_cap) {
-            if (grow[0] + 1024 <= c->pool_cap / 4 * 3) {
+        // a hinted next batch is gathered into the free HBM above this merge: keep room for about
+        // its endpoint rows (two per edit at the average degree, at most half the pool)
+        long long headroom = 0;
+        if (c->pf_pending && c->pf_m > 0) {
+            const long long avg = c->n > 0 ? (c->nnz + c->n - 1) / c->n : 1;
+            headroom = std::min<long long>(c->pool_cap / 2, 2 * c->pf_m * avg + 4096);
+        }
+        if (c->tail + grow[0] + 1024 + headroom > c->pool_cap) {
+            if (grow[0] + 1024 + headroom <= c->pool_cap / 4 * 3) {
+                SCOUT_RC(graph_compact(c, grow[0] + 1024 + headroom, true));
+            } else if (c->tail + grow[0] + 1024 <= c->pool_cap) {
+                // the gather gets what is left
+            } else if (grow[0] + 1024 <= c->pool_cap / 4 * 3) {
                 SCOUT_RC(graph_compact(c, grow[0] + 1024, true));
             } else {
                 c->batch_dest = 1;
