@@ -18,7 +18,7 @@ struct DevCounters {
     int n_del;          // edits classified as deletions
     int n_half;         // applied half-edits (2 per applied edit)
     int n_aff;          // vertices whose row changed
-    int n_small, n_large;     // rows planned by a warp / by a block
+    int n_small, n_large;     // rows of the short-row merge / long rows compacted in place
     int n_slices, n_pad;      // merge slices
     long long new_elems;      // elements written to the pool this batch (HBM part when split)
     long long new_elems_host; // tiered store, split batch: elements written to the host pool
@@ -144,6 +144,7 @@ struct scout_ctx {
     int64_t* d_aff_len = nullptr;   // new length, then exclusive offsets (2m + 1)
     int64_t* d_aff_len2 = nullptr;  // tiered split batches: lengths / offsets of the host rows (2m + 1)
     int32_t* d_aff_small = nullptr; // affected rows merged by the short-row merge (2m)
+    int32_t* d_aff_long = nullptr;  // long affected rows compacted in place (2m)
     int64_t* d_small_off = nullptr; // short-row lengths, then their exclusive scan (2m + 1)
     scout::Row* d_old_row = nullptr;   // descriptors of the affected rows before the batch (2m)
     int64_t* d_slices = nullptr;  int64_t cap_slices = 0;   // merge items (row << 32 | slice)

@@ -80,7 +80,21 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather_copy(Row* __restrict_
         const Row r = row[x];
         const int32_t* s = pool + r.start;
         int32_t* d = pool + dst[k];
-        for (int j = (int)lane_id(); j < r.len; j += WARP) d[j] = s[j];
+        // four loads in flight per lane before their stores (reads cross the host link)
+        constexpr int U = 4;
+        for (int j0 = 0; j0 < r.len; j0 += U * WARP) {
+            int32_t v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u * WARP + (int)lane_id();
+                v[u] = j < r.len ? s[j] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u * WARP + (int)lane_id();
+                if (j < r.len) d[j] = v[u];
+            }
+        }
         moved += r.len;
         __syncwarp();
         __threadfence();   // the entries are visible before the descriptor points at them

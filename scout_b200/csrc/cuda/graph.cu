@@ -36,10 +36,12 @@ namespace scout {
 constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the long-row merge
 constexpr int SMALL_LEN = 2048;      // rows up to this length go to the short-row merge
 
-// A short row whose half-edits are all deletions is rewritten in place: its survivors only
-// move towards the row start, it keeps its start and capacity, and it takes no pool space.
+// A row whose half-edits are all deletions is rewritten in place: its survivors only move
+// towards the row start, it keeps its start and capacity, and it takes no pool space (short
+// rows in the short-row merge, longer ones by one block each in k_merge_long_inplace).
 __host__ __device__ __forceinline__ bool in_place_row(long long insertions, int old_len) {
-    return insertions == 0 && old_len <= SMALL_LEN;
+    (void)old_len;
+    return insertions == 0;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -233,22 +235,26 @@ __device__ __forceinline__ long long warp_lower_bound(const int64_t* a, long lon
 __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
                             const int64_t* __restrict__ seg, Row* __restrict__ old_row, int64_t* __restrict__ alloc,
                             int32_t* __restrict__ small, int64_t* __restrict__ small_len, int64_t* __restrict__ slices,
-                            int64_t slice_cap) {
+                            int64_t slice_cap, int32_t* __restrict__ longs) {
     const int A = ctr->n_aff;
     const int T = gridDim.x * blockDim.x;
     for (int b = (int)(blockIdx.x * blockDim.x + threadIdx.x) - (int)lane_id(); b < A; b += T) {
         const int a = b + (int)lane_id();
         const bool ok = a < A;
         int ns = 0;
-        bool sm = false;
+        bool sm = false, lip = false;
         if (ok) {
             const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
             const Row r = row[aff[a]];
             old_row[a] = r;
-            alloc[a] = in_place_row(sp - b0, r.len) ? 0 : (long long)r.len + (sp - b0);
+            const bool ip = in_place_row(sp - b0, r.len);
+            alloc[a] = ip ? 0 : (long long)r.len + (sp - b0);
             sm = r.len <= SMALL_LEN;
-            ns = sm ? 0 : (r.len + SLICE - 1) / SLICE;
+            lip = !sm && ip;   // a long row that only loses entries: compacted in place by one block
+            ns = sm || lip ? 0 : (r.len + SLICE - 1) / SLICE;
         }
+        const int lat = warp_append(lip, &ctr->n_large);
+        if (lip) longs[lat] = a;
         const int at = warp_append(ok && sm, &ctr->n_small);
         if (ok && sm) {
             small[at] = a;
@@ -465,6 +471,56 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
                     __syncwarp();
                 }
             }
+        }
+    }
+}
+
+// Long rows that only lose entries, compacted in place: one block per row streams it front to
+// back in chunks of LIP_CHUNK entries; every entry of a chunk is loaded before any survivor
+// of that chunk is stored, and a survivor's new position (survivors before it in the row)
+// never exceeds its old one, so no store lands on an entry still to be read.
+constexpr int LIP_THREADS = 256;
+constexpr int LIP_U = 4;
+constexpr int LIP_CHUNK = LIP_THREADS * LIP_U;
+
+__global__ void __launch_bounds__(LIP_THREADS) k_merge_long_inplace(int32_t* __restrict__ pool,
+                                                                    const DevCounters* __restrict__ ctr,
+                                                                    const int32_t* __restrict__ longs,
+                                                                    const Row* __restrict__ old_row) {
+    __shared__ int s_warp[LIP_U][LIP_THREADS / WARP];
+    const int t = threadIdx.x, w = t / WARP;
+    const unsigned lt = (1u << lane_id()) - 1;
+    const int nl = ctr->n_large;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        const Row r = old_row[longs[li]];
+        int32_t* O = pool + r.start;
+        long long run = 0;
+        for (long long b = 0; b < r.len; b += LIP_CHUNK) {
+            int32_t x[LIP_U];
+            unsigned m[LIP_U];
+#pragma unroll
+            for (int u = 0; u < LIP_U; u++) {
+                const long long i = b + u * LIP_THREADS + t;
+                x[u] = i < r.len ? O[i] : -1;
+                m[u] = __ballot_sync(0xffffffffu, x[u] >= 0);
+                if (lane_id() == 0) s_warp[u][w] = __popc(m[u]);
+            }
+            __syncthreads();   // every load of the chunk is done; the warp counts are visible
+            long long base = run;
+#pragma unroll
+            for (int u = 0; u < LIP_U; u++) {
+                int before = 0, total = 0;
+#pragma unroll
+                for (int k = 0; k < LIP_THREADS / WARP; k++) {
+                    const int cnt = s_warp[u][k];
+                    before += k < w ? cnt : 0;
+                    total += cnt;
+                }
+                if (x[u] >= 0) O[base + before + __popc(m[u] & lt)] = x[u];
+                base += total;
+            }
+            run = base;
+            __syncthreads();   // the counts are read before the next chunk overwrites them
         }
     }
 }
@@ -818,7 +874,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
         (size_t)M * sizeof(scout_edge), (size_t)M, (size_t)M,
         (size_t)H * 8, (size_t)H * 8, (size_t)(H + 1) * 8,
         (size_t)H * 4, (size_t)3 * H * 8, (size_t)(H + 1) * 8, (size_t)H * 4, (size_t)(H + 1) * 8, (size_t)H * sizeof(Row),
-        (size_t)(H + 1) * 8};
+        (size_t)(H + 1) * 8, (size_t)H * 4};
     size_t total = 0;
     for (size_t s : sz) total += align256(s);
     if (c->ws) dev_free(c, c->ws, (size_t)c->ws_bytes);
@@ -842,6 +898,7 @@ int ws_ensure(scout_ctx* c, int64_t m) {
     c->d_small_off = (int64_t*)take(sz[10]);
     c->d_old_row = (Row*)take(sz[11]);
     c->d_aff_len2 = (int64_t*)take(sz[12]);
+    c->d_aff_long = (int32_t*)take(sz[13]);
     c->d_hkeys = c->d_keys;
     return SCOUT_OK;
 }
@@ -1174,7 +1231,8 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
         if (again) SCOUT_CU(c, cudaMemsetAsync(&c->d_ctr->n_small, 0, 4 * sizeof(int), c->s_main));   // n_small .. n_pad
         k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg,
                                                                   c->d_old_row, c->d_aff_len, c->d_aff_small,
-                                                                  c->d_small_off, c->d_slices, c->cap_slices);
+                                                                  c->d_small_off, c->d_slices, c->cap_slices,
+                                                                  c->d_aff_long);
         SCOUT_LAUNCH(c, "k_row_alloc");
         c->nlaunch += 1;
         if (split) {
@@ -1262,11 +1320,13 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     k_merge_small<<<blocks_for(groups * WARP, MERGE_THREADS), MERGE_THREADS, 0, c->s_main>>>(
         c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, dest, c->d_aff_small,
         c->d_small_off);
+    k_merge_long_inplace<<<(unsigned)std::min<int64_t>(std::max<int64_t>(1, Amax), 8 * (int64_t)c->sm_count),
+                           LIP_THREADS, 0, c->s_main>>>(c->pool, c->d_ctr, c->d_aff_long, c->d_old_row);
     k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, MS_THREADS), MS_THREADS,
                      0, c->s_main>>>(c->pool, (long long)c->pool_cap, sorted, B, c->d_ctr, c->d_aff_seg,
                                      c->d_old_row, c->d_aff_len, dest, E, dpos, c->d_slices, c->cap_slices);
     SCOUT_LAUNCH(c, "merge");
-    c->nlaunch += 5;
+    c->nlaunch += 6;
     return SCOUT_OK;
 }
 
