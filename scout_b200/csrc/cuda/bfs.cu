@@ -25,9 +25,6 @@
 namespace scout {
 
 constexpr int BFS_THREADS = 256;
-constexpr int CAND_LANES = 8;                   // lanes per short row in the invalidation and seed passes
-constexpr int CAND_GROUPS = WARP / CAND_LANES;  // short rows per warp at once
-constexpr int SEED_SHORT = 64;                  // seed items up to this length go to a lane group
 
 struct BfsParams {
     DGraph g;
@@ -481,91 +478,56 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
             const int nxt = (cur + 1) % 3, zer = (cur + 2) % 3;
             if (leader) p.ctr->q_count[zer] = 0;
             tag++;
-            // Candidates of this round. A candidate whose row fits one queue item (the common,
-            // short case) is decided by a group of CAND_LANES lanes, CAND_GROUPS rows per warp at
-            // once: the group looks for a valid parent and, when there is none, invalidates the
-            // vertex and pushes its children (the pushes are warp-collective, so every lane takes
-            // part in the longest group's steps). Each chunk of a long row is then checked by the
-            // whole warp (found = tag marks a chunk holding a parent).
-            for (int i0 = wid * CAND_GROUPS; i0 < cnt; i0 += W * CAND_GROUPS) {
-                const int grp = (int)lane_id() / CAND_LANES, gl = (int)lane_id() % CAND_LANES;
-                const unsigned gmask = ((1u << CAND_LANES) - 1u) << (grp * CAND_LANES);
-                const int i = i0 + grp;
-                int32_t c = 0;
-                int chunk = 0, lc = 0, clen = 0;
-                long long rs = 0;
-                bool big = false, live = false;
-                if (i < cnt) {
-                    const unsigned long long item = p.q[cur][i];
-                    c = (int32_t)(item & 0xffffffffu);
-                    chunk = (int)(item >> 32);
-                    const Row r = p.g.row[c];
-                    big = r.len > p.chunk;
-                    lc = ld_level(p.level + c);
-                    live = !(c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch);
-                    if (!live && big && gl == 0) p.found[c] = (int32_t)tag;   // nothing to decide
-                    const long long c0 = (long long)chunk << p.chunk_log2;
-                    clen = (int)max(0LL, min((long long)p.chunk, (long long)r.len - c0));
-                    rs = r.start + c0;
+            for (int i = wid; i < cnt; i += W) {
+                const unsigned long long item = p.q[cur][i];
+                const int32_t c = (int32_t)(item & 0xffffffffu);
+                const int chunk = (int)(item >> 32);
+                const Row r = p.g.row[c];
+                const bool big = r.len > p.chunk;
+                const int lc = ld_level(p.level + c);
+                if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) {
+                    if (big && lane_id() == 0) p.found[c] = (int32_t)tag;   // nothing to decide
+                    continue;
                 }
-                const bool mine = live && !big;
+                const long long c0 = ((long long)chunk << p.chunk_log2);
+                const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
+                const int32_t* rw = p.g.pool + r.start + c0;
                 bool found = false;
-                const int steps = __reduce_max_sync(0xffffffffu, mine ? (clen + CAND_LANES - 1) / CAND_LANES : 0);
-                for (int st = 0; st < steps; st++) {
-                    const int k = st * CAND_LANES + gl;
+                for (int b0 = 0; b0 < clen && !found; b0 += WARP) {
+                    int k = b0 + (int)lane_id();
                     bool ok = false;
-                    if (mine && !found && k < clen) {
-                        const int32_t w = p.g.pool[rs + k];
+                    if (k < clen) {
+                        int32_t w = rw[k];
                         ok = ld_level(p.level + w) == lc - 1 && ld_volatile(p.st_inval + w) != p.epoch;
-                        bytes += 8;
                     }
-                    found = found || (__ballot_sync(0xffffffffu, ok) & gmask) != 0;
-                    if (__all_sync(0xffffffffu, !mine || found)) break;
+                    found = __any_sync(0xffffffffu, ok);
+                    if (k < clen) bytes += 8;
                 }
-                const bool inv = mine && !found;
-                if (inv && gl == 0) {
+                if (big) {
+                    if (lane_id() == 0) {
+                        if (found) p.found[c] = (int32_t)tag;
+                        if (chunk == 0) p.ctr->list_count[2] = 1;   // a long candidate this round
+                    }
+                    continue;
+                }
+                if (found) continue;
+                if (lane_id() == 0) {
                     p.st_inval[c] = p.epoch;
-                    const int at = atomicAdd(&p.ctr->list_count[0], 1);
+                    int at = atomicAdd(&p.ctr->list_count[0], 1);
                     p.inval[at] = c;
                 }
                 __syncwarp();
-                const int psteps = __reduce_max_sync(0xffffffffu, inv ? (clen + CAND_LANES - 1) / CAND_LANES : 0);
-                for (int st = 0; st < psteps; st++) {
-                    const int k = st * CAND_LANES + gl;
+                for (int b0 = 0; b0 < clen; b0 += WARP) {
+                    int k = b0 + (int)lane_id();
                     bool ch = false;
                     int32_t w = 0;
-                    if (inv && k < clen) {
-                        w = p.g.pool[rs + k];
+                    if (k < clen) {
+                        w = rw[k];
                         ch = ld_level(p.level + w) == lc + 1 && ld_volatile(p.st_inval + w) != p.epoch;
                     }
                     push_vertex(p, ch, w, nxt, tag, true, false);
                 }
-                if (inv && gl == 0) bytes += 8LL * clen + 24;
-                unsigned bigm = __ballot_sync(0xffffffffu, live && big && gl == 0);
-                while (bigm) {
-                    const int j = __ffs(bigm) - 1;
-                    bigm &= bigm - 1;
-                    const int32_t cj = __shfl_sync(0xffffffffu, c, j);
-                    const int chj = __shfl_sync(0xffffffffu, chunk, j);
-                    const int lcj = __shfl_sync(0xffffffffu, lc, j);
-                    const int lenj = __shfl_sync(0xffffffffu, clen, j);
-                    const long long rsj = __shfl_sync(0xffffffffu, rs, j);
-                    bool fj = false;
-                    for (int b0 = 0; b0 < lenj && !fj; b0 += WARP) {
-                        const int k = b0 + (int)lane_id();
-                        bool ok = false;
-                        if (k < lenj) {
-                            const int32_t w = p.g.pool[rsj + k];
-                            ok = ld_level(p.level + w) == lcj - 1 && ld_volatile(p.st_inval + w) != p.epoch;
-                            bytes += 8;
-                        }
-                        fj = __any_sync(0xffffffffu, ok);
-                    }
-                    if (lane_id() == 0) {
-                        if (fj) p.found[cj] = (int32_t)tag;
-                        if (chj == 0) p.ctr->list_count[2] = 1;   // a long candidate this round
-                    }
-                }
+                if (lane_id() == 0) bytes += 8LL * clen + 24;
             }
             if (!grid_sync(p.bar, 3)) return;
             if (ld_volatile(&p.ctr->list_count[2])) {
@@ -637,77 +599,36 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
         }
         if (!grid_sync(p.bar, 5)) return;
         tag++;
-        // boundary seeds: every chunk of an invalidated vertex's row offers (min level of its
-        // valid neighbours) + 1. Chunks of up to SEED_SHORT entries are reduced by a group of
-        // CAND_LANES lanes (CAND_GROUPS per warp at once), longer ones by the whole warp.
+        // boundary seeds: warp per chunk of an invalidated vertex's row
         const int nseed = qcount(p, 2);
-        for (int i0 = wid * CAND_GROUPS; i0 < nseed; i0 += W * CAND_GROUPS) {
-            const int grp = (int)lane_id() / CAND_LANES, gl = (int)lane_id() % CAND_LANES;
-            const int i = i0 + grp;
-            int32_t c = 0;
-            int clen = 0;
-            long long rs = 0;
-            if (i < nseed) {
-                const unsigned long long item = p.q[2][i];
-                c = (int32_t)(item & 0xffffffffu);
-                const Row r = p.g.row[c];
-                const long long c0 = ((long long)(item >> 32) << p.chunk_log2);
-                clen = (int)max(0LL, min((long long)p.chunk, (long long)r.len - c0));
-                rs = r.start + c0;
-            }
-            const bool small = i < nseed && clen <= SEED_SHORT;
+        for (int i = wid; i < nseed; i += W) {
+            const unsigned long long item = p.q[2][i];
+            const int32_t c = (int32_t)(item & 0xffffffffu);
+            const Row r = p.g.row[c];
+            const long long c0 = ((long long)(item >> 32) << p.chunk_log2);
+            const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
+            const int32_t* rw = p.g.pool + r.start + c0;
             unsigned best = 0xffffffffu;
-            const int steps = __reduce_max_sync(0xffffffffu, small ? (clen + CAND_LANES - 1) / CAND_LANES : 0);
-            for (int st = 0; st < steps; st++) {
-                const int k = st * CAND_LANES + gl;
-                if (small && k < clen) {
-                    const int32_t w = p.g.pool[rs + k];
+            for (int b0 = 0; b0 < clen; b0 += WARP) {
+                int k = b0 + (int)lane_id();
+                if (k < clen) {
+                    int32_t w = rw[k];
                     if (ld_volatile(p.st_inval + w) != p.epoch) {
-                        const int lw = ld_level(p.level + w);
+                        int lw = ld_level(p.level + w);
                         if (lw >= 0) best = min(best, (unsigned)lw);
                     }
                 }
             }
 #pragma unroll
-            for (int o = CAND_LANES / 2; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+            for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane_id() == 0) bytes += 8LL * max(clen, 0) + 24;
             bool dec = false;
-            if (small && gl == 0) {
-                bytes += 8LL * clen + 24;
-                if (best != 0xffffffffu) {
-                    const unsigned cand = best + 1;
-                    dec = atomicMin((unsigned*)(p.level + c), cand) > cand;
-                }
+            if (lane_id() == 0 && best != 0xffffffffu) {
+                unsigned cand = best + 1;
+                unsigned old = atomicMin((unsigned*)(p.level + c), cand);
+                dec = old > cand;
             }
             push_vertex(p, dec, c, 0, tag, true, false);
-            unsigned bigm = __ballot_sync(0xffffffffu, i < nseed && !small && gl == 0);
-            while (bigm) {
-                const int j = __ffs(bigm) - 1;
-                bigm &= bigm - 1;
-                const int32_t cj = __shfl_sync(0xffffffffu, c, j);
-                const int lenj = __shfl_sync(0xffffffffu, clen, j);
-                const long long rsj = __shfl_sync(0xffffffffu, rs, j);
-                unsigned bj = 0xffffffffu;
-                for (int b0 = 0; b0 < lenj; b0 += WARP) {
-                    const int k = b0 + (int)lane_id();
-                    if (k < lenj) {
-                        const int32_t w = p.g.pool[rsj + k];
-                        if (ld_volatile(p.st_inval + w) != p.epoch) {
-                            const int lw = ld_level(p.level + w);
-                            if (lw >= 0) bj = min(bj, (unsigned)lw);
-                        }
-                    }
-                }
-                bj = __reduce_min_sync(0xffffffffu, bj);
-                bool dj = false;
-                if (lane_id() == 0) {
-                    bytes += 8LL * lenj + 24;
-                    if (bj != 0xffffffffu) {
-                        const unsigned cand = bj + 1;
-                        dj = atomicMin((unsigned*)(p.level + cj), cand) > cand;
-                    }
-                }
-                push_vertex(p, dj, cj, 0, tag, true, false);
-            }
         }
         // insertion seeds: thread per half-edit
         for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
