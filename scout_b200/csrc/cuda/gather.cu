@@ -124,11 +124,13 @@ int gather_launch(scout_ctx* c, long long base) {
     SCOUT_CU(c, cudaMemsetAsync(c->d_gctr, 0, sizeof(GatherCtr), s));
     SCOUT_CU(c, cudaMemcpyAsync(c->d_pf_edits, c->h_pf_edits, (size_t)m * sizeof(scout_edge), cudaMemcpyHostToDevice, s));
     c->gather_tag = c->gather_tag + 1 == 0 ? 1 : c->gather_tag + 1;
-    k_gather_plan<<<blocks_for(2 * m, GATHER_THREADS), GATHER_THREADS, 0, s>>>(
+    k_gather_plan<<<blocks_for(2 * m, GATHER_THREADS, c->sm_count), GATHER_THREADS, 0, s>>>(
         c->row, (int32_t)c->n, c->d_pf_edits, m, (long long)c->pool_cap, c->gather_stamp, (int32_t)c->gather_tag, base, room,
         c->d_gather_list, c->d_gather_dst, (GatherCtr*)c->d_gctr);
-    k_gather_copy<<<4 * c->sm_count, GATHER_THREADS, 0, s>>>(c->row, c->pool, c->d_gather_list, c->d_gather_dst,
-                                                             (GatherCtr*)c->d_gctr);
+    // one block per SM: the copy is bound by the host link, and the repair's persistent kernel
+    // (up to four 256-thread blocks per SM) must still fit beside it to run concurrently
+    k_gather_copy<<<c->sm_count, GATHER_THREADS, 0, s>>>(c->row, c->pool, c->d_gather_list, c->d_gather_dst,
+                                                         (GatherCtr*)c->d_gctr);
     SCOUT_LAUNCH(c, "gather");
     c->nlaunch += 2;
     SCOUT_CU(c, cudaMemcpyAsync(c->h_gctr, c->d_gctr, sizeof(GatherCtr), cudaMemcpyDeviceToHost, s));
