@@ -303,7 +303,8 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
         e0, e1 = st.pop("_ev")
         st["ms_step"] = e0.elapsed_time(e1)
         if verbose:
-            keep = ("edits", "ms_step", "ms_h2d", "ms_update", "ms_repair", "rounds", "changed", "launches", "variant")
+            keep = ("edits", "ms_step", "ms_h2d", "ms_update", "ms_repair", "rounds", "changed", "launches", "variant",
+                    "hbm_bytes", "update_bytes")
             d = {k: (round(st[k], 3) if isinstance(st[k], float) else st[k]) for k in keep}
             d["phase_ms"] = [round(x, 3) for x in st["phase_ms"]]
             print(problem, json.dumps(d), file=sys.stderr, flush=True)
@@ -531,7 +532,8 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
                 else:
                     ctx.load_csr(off, adj)
                 ctx.upload(p, init)
-                sched = dict(tuned.get(p, {}))
+                # the plain arms run the default knobs; the others the autotuned ones
+                sched = {} if arm in ("tiered_plain", "in_hbm_plain") else dict(tuned.get(p, {}))
                 if mdl is not None:
                     ctx.sched_install(p, mdl)
                     sched["policy"] = 1

@@ -130,9 +130,19 @@ def tune_rounds(problem, streams, arrivals, device: int = 0, caps=CAPS, sched=No
             wall = 1e3 * (time.perf_counter() - t0)
         table.append({"round_cap": cap, "rounds": len(rounds), "device_ms": dev, "wall_ms": wall,
                       "p99_batch_ms": float(np.percentile(lat, 99))})
+    return {"problem": problem, "p99_bound_ms": p99_ms, "best": {"round_cap": choose_round_cap(table, p99_ms)},
+            "table": table}
+
+
+def choose_round_cap(table, p99_ms: float, slack: float = 0.05) -> int:
+    """Among the caps whose p99 batch latency stays within p99_ms, the smallest one whose total
+    wall time is within `slack` of the fastest (bigger rounds that barely raise throughput only
+    add latency); the smallest cap when none meets the bound."""
     ok = [r for r in table if r["p99_batch_ms"] <= p99_ms]
-    best = min(ok, key=lambda r: r["wall_ms"]) if ok else min(table, key=lambda r: r["round_cap"])
-    return {"problem": problem, "p99_bound_ms": p99_ms, "best": {"round_cap": best["round_cap"]}, "table": table}
+    if not ok:
+        return min(r["round_cap"] for r in table)
+    fastest = min(r["wall_ms"] for r in ok)
+    return min(r["round_cap"] for r in ok if r["wall_ms"] <= (1 + slack) * fastest)
 
 
 def main():

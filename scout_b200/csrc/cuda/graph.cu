@@ -1263,13 +1263,14 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
             return SCOUT_OK;
         };
         SCOUT_RC(read_grow());
-        // a hinted next batch is gathered into the free HBM above this merge: keep room for its
-        // endpoint rows (two per edit; endpoints drawn by degree have rows far above the average,
-        // so sixteen times the average degree each), at most half the pool
+        // a hinted next batch is gathered into the free HBM above this merge: keep room for about
+        // its endpoint rows at the average degree (two per edit), at most a quarter of the pool.
+        // More room means evicting more rows to the host pool on every compaction, which costs
+        // more over the host link than the merge saves on the gathered rows.
         long long headroom = 0;
         if (c->pf_pending && c->pf_m > 0) {
             const long long avg = c->n > 0 ? (c->nnz + c->n - 1) / c->n : 1;
-            headroom = std::min<long long>(c->pool_cap / 2, 32 * c->pf_m * avg + 4096);
+            headroom = std::min<long long>(c->pool_cap / 4, 2 * c->pf_m * avg + 4096);
         }
         if (c->tail + grow[0] + 1024 + headroom > c->pool_cap) {
             if (grow[0] + 1024 + headroom <= c->pool_cap / 4 * 3) {

@@ -104,3 +104,50 @@ def test_union_equals_streams_alone(problem, learned):
                     assert orc.check_mis(o, a, got) == (0, 0)
         for c in singles:
             c.close()
+
+
+@pytest.mark.parametrize("problem", ["bfs", "cc", "coloring", "mis"])
+def test_union_with_a_large_stream(problem):
+    """A stream on an R-MAT scale-19 graph (about 16 M directed entries) with a 10^6-edit batch
+    shares rounds with two small streams; every stream equals its single-stream run and, for
+    BFS and CC, the ground truth of its current graph."""
+    specs = [(19, 16, sb.STREAM_PREFERENTIAL, [1_000_000, 2000]), (14, 16, sb.STREAM_MIXED, [500, 20000]),
+             (12, 8, sb.STREAM_PREFERENTIAL, [100, 100])]
+    streams = []
+    for i, (sc, ef, kind, sizes) in enumerate(specs):
+        h = sb.gen_rmat(sc, ef, seed=70 + i)
+        off, adj = h.arrays()
+        s = h.stream(kind, sum(sizes), 1, insert_ratio=0.5, seed=170 + i)
+        b = np.cumsum([0] + sizes)
+        streams.append((off, adj, [np.ascontiguousarray(s[b[j]:b[j + 1]]) for j in range(len(sizes))]))
+    arrivals = [(sid, streams[sid][2][j]) for j in range(2) for sid in (0, 1, 2)]
+    rounds = sb.form_rounds(arrivals, 1 << 21)
+    with sb.MultiEngine(problem) as me:
+        singles, truths = [], []
+        for off, adj, _ in streams:
+            init = _init(problem, off, adj)
+            me.add_stream(off, adj, init, 0)
+            ctx = sb.Context(0)
+            ctx.load_csr(off, adj)
+            ctx.upload(problem, init)
+            singles.append(ctx)
+            truths.append(orc.Graph(off, adj))
+        me.reserve_batches(1 << 21)
+        for rd in rounds:
+            me.round(rd)
+            for sid, b in rd:
+                singles[sid].repair(problem, b)
+                got = me.download(sid)
+                assert np.array_equal(got, singles[sid].download(problem)), f"stream {sid} differs"
+                truths[sid].toggle_batch(b)
+                o, a = truths[sid].csr()
+                if problem == "bfs":
+                    assert np.array_equal(got, orc.gt_bfs(o, a, 0))
+                elif problem == "cc":
+                    assert np.array_equal(got, orc.gt_cc(o, a))
+                elif problem == "coloring":
+                    assert orc.check_coloring(o, a, got) == 0
+                else:
+                    assert orc.check_mis(o, a, got) == (0, 0)
+        for c in singles:
+            c.close()
