@@ -247,6 +247,16 @@ def load_model(path):
     return {k: np.asarray(d[k], dtype=np.float32) for k in ("bfs", "cc") if k in d.files}
 
 
+LAUNCH_KNOBS = ("blocks_per_sm", "chunk_log2", "lanes_per_vertex")
+
+
+def launch_knobs(knobs: dict) -> dict:
+    """The launch knobs of a tuned set, without its plain repair variant (mode, frontier): that
+    choice was tuned on one stream of the headline workload; union rounds and tiered batches
+    leave the variant to the plain default or the learned scheduler."""
+    return {k: v for k, v in (knobs or {}).items() if k in LAUNCH_KNOBS}
+
+
 def load_tuned(path):
     """Autotuned knobs: {problem: {"blocks_per_sm", "chunk_log2"}, "round_cap": int}, or {}."""
     if not path or not os.path.exists(path):
@@ -533,7 +543,7 @@ def out_of_core(a, device, model, tuned, nbatches: int = 6, m: int = 1_000_000):
                     ctx.load_csr(off, adj)
                 ctx.upload(p, init)
                 # the plain arms run the default knobs; the others the autotuned ones
-                sched = {} if arm in ("tiered_plain", "in_hbm_plain") else dict(tuned.get(p, {}))
+                sched = {} if arm in ("tiered_plain", "in_hbm_plain") else launch_knobs(tuned.get(p, {}))
                 if mdl is not None:
                     ctx.sched_install(p, mdl)
                     sched["policy"] = 1
@@ -680,7 +690,7 @@ def multi_stream(a, device, model, tuned):
             me.seal()
             cap = int(tuned.get("round_cap", 1 << 21))
             me.reserve_batches(max(cap, max(len(pinned[(i, j)]) for i, j in arr_p)))
-            sched = dict(tuned.get(p, {}))
+            sched = launch_knobs(tuned.get(p, {}))
             if mdl is not None and p in mdl:
                 me.context.sched_install(p, mdl[p])
                 sched["policy"] = 1
