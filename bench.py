@@ -281,9 +281,14 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
         sched["policy"] = 1
     ctx.reserve_batches(max(len(b) for b in batches))   # no allocation inside the timed loop
     mirror = init.copy()
-    # each step's edits are read from page-locked host memory (copied there before timing)
+    # each step's edits are read from page-locked host memory (copied there before timing); the
+    # next step's edits are hinted (prefetch) so that their host-to-device copy overlaps this
+    # step's repair, as a stream consumer that knows its next batch does
     batches = [sb.pinned_copy(b) for b in batches[:warmup + steps]]
-    for b in batches[:warmup]:
+    nb = len(batches)
+    for i, b in enumerate(batches[:warmup]):
+        if i + 1 < nb:
+            ctx.prefetch(batches[i + 1])
         ctx.repair(problem, b, sched=sched)
         ctx.commit(problem, mirror)
     timed = batches[warmup:warmup + steps]
@@ -294,10 +299,12 @@ def run_problem(problem, off, adj, init, batches, warmup, steps, device, dist, c
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks.start()
     ev0.record()
-    for b in timed:
+    for i, b in enumerate(timed):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
+        if i + 1 < len(timed):
+            ctx.prefetch(timed[i + 1])
         st = ctx.repair(problem, b, sched=sched)
         changed = ctx.commit(problem, mirror)
         e1.record()

@@ -74,7 +74,12 @@ typedef struct scout_sched {
     int32_t blocks_per_sm;    /* persistent repair kernels: resident blocks per SM (1..4;
                                  0 = as many as fit, at most 4)                          */
     int32_t chunk_log2;       /* BFS queue item = 2^chunk_log2 row entries (8..13; 0 = 10) */
-    int64_t reserved[2];
+    int32_t prefetched;       /* 1: this call's edits (same count, no ops) are the batch given
+                                 to the last scout_prefetch; the device copy that the previous
+                                 scout_repair started is used instead of a new upload (when
+                                 there is none, or the count differs, the edits are uploaded) */
+    int32_t pad0;
+    int64_t reserved[1];
 } scout_sched;
 
 /* Per-batch statistics (the fields of the reference's Stats structs, scout_bfs.cu:417-424,
@@ -202,14 +207,16 @@ int scout_repair_bfs(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops
                      const scout_sched* sched, scout_batch_stats* stats);
 int scout_repair_cc(scout_ctx* ctx, const scout_edge* edits, const uint8_t* ops, int64_t m,
                     const scout_sched* sched, scout_batch_stats* stats);
-/* Hint: the edits of the batch that will follow the next scout_repair call (copied; the
- * caller's buffer is free on return). On a tiered store, that repair call, once its own merge
- * is done, gathers the rows of these edits' endpoints that are still in host memory into free
- * HBM on a copy stream while its repair runs, so the hinted batch's merge and repair find
- * them in HBM (its stats report the gather). The fetch of batch K+1 overlapping the repair of
- * batch K replaces the reference's per-round host fetch (scout_bfs.cu:199-229) and MIS's
- * K+1 || K channels (scout_mis.cu:855-912). On an all-HBM store it does nothing. A hint
- * that does not match the next batch only costs the copy. */
+/* Hint: the edits of the batch that will follow the next scout_repair call. That repair call,
+ * once its own merge is queued, copies them to the device on a copy stream while its repair
+ * runs; the following scout_repair that declares them (scout_sched.prefetched = 1) reads that
+ * copy instead of uploading its edits. On a tiered store the same call also gathers the rows
+ * of these edits' endpoints that are still in host memory into free HBM, so the hinted batch's
+ * merge and repair find them in HBM (its stats report the gather). A page-locked `next` is
+ * read in place by that copy and must stay unchanged until the repair that uses it; other
+ * buffers are copied here and are free on return. The fetch of batch K+1 overlapping the
+ * repair of batch K replaces the reference's per-round host fetch (scout_bfs.cu:199-229) and
+ * MIS's K+1 || K channels (scout_mis.cu:855-912). A hint that is not used only costs the copy. */
 int scout_prefetch(scout_ctx* ctx, const scout_edge* next, int64_t m);
 /* Commit of the last repair's changed entries into a host mirror of n entries: the device
  * gathers (id, value) pairs of changed entries and copies them back; the host scatters

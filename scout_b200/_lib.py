@@ -28,7 +28,8 @@ class ScoutEdge(C.Structure):
 class ScoutSched(C.Structure):
     _fields_ = [("policy", C.c_int32), ("mode", C.c_int32), ("frontier", C.c_int32),
                 ("lanes_per_vertex", C.c_int32), ("search_bound", C.c_int64), ("search_limit", C.c_int64),
-                ("blocks_per_sm", C.c_int32), ("chunk_log2", C.c_int32), ("reserved", C.c_int64 * 2)]
+                ("blocks_per_sm", C.c_int32), ("chunk_log2", C.c_int32), ("prefetched", C.c_int32),
+                ("pad0", C.c_int32), ("reserved", C.c_int64 * 1)]
 
 
 class ScoutBatchStats(C.Structure):

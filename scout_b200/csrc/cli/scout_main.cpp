@@ -203,17 +203,22 @@ int main(int argc, char** argv) {
     long long tot_ins_eff = 0, tot_del_eff = 0, tot_recomputed_del = 0, batches_recomputed = 0;
     double kernel_ms = 0, transfer_ms = 0;
     std::vector<int32_t> before;
+    bool hinted = false;   // the current batch was passed to scout_prefetch
     for (size_t i = 0; i < batches.size(); i++) {
         auto& b = batches[i];
         scout_batch_stats st;
         auto t0 = clk::now();
-        // the next batch's cold rows (a graph beyond the device budget) are gathered during this
-        // repair, as the reference's MIS pipeline prepares batch K+1 while K runs
-        // (scout_mis.cu:855-912); a graph held wholly in HBM ignores the hint
-        if (i + 1 < batches.size() && !batches[i + 1].empty())
-            scout_prefetch(ctx, batches[i + 1].data(), (int64_t)batches[i + 1].size());
+        // the next batch's edits are copied to the device during this repair (and, for a graph
+        // beyond the device budget, its cold rows gathered into HBM), as the reference's MIS
+        // pipeline prepares batch K+1 while K runs (scout_mis.cu:855-912); the next repair then
+        // declares them prefetched (toggle batches: explicit ops are uploaded with the edits)
+        scout_sched sd;
+        std::memset(&sd, 0, sizeof(sd));
+        sd.prefetched = hinted && ops[i].empty() ? 1 : 0;
+        hinted = i + 1 < batches.size() && !batches[i + 1].empty();
+        if (hinted) scout_prefetch(ctx, batches[i + 1].data(), (int64_t)batches[i + 1].size());
         int rc = scout_repair(ctx, problem, b.data(), ops[i].empty() ? nullptr : ops[i].data(), (int64_t)b.size(),
-                              nullptr, &st);
+                              &sd, &st);
         if (rc != SCOUT_OK) die("repair failed", scout_last_error(ctx));
         auto t1 = clk::now();
         if (dump_touched) before = sol;

@@ -85,7 +85,8 @@ static void release(scout_ctx* c) {
     for (int i = 0; i < 8; i++) if (c->ev_t[i]) cudaEventDestroy(c->ev_t[i]);
     if (c->ev_gather0) cudaEventDestroy(c->ev_gather0);
     if (c->ev_gather1) cudaEventDestroy(c->ev_gather1);
-    void* gdev[] = {c->gather_stamp, c->d_gctr, c->d_pf_edits, c->d_gather_list, c->d_gather_dst};
+    if (c->ev_pf) cudaEventDestroy(c->ev_pf);
+    void* gdev[] = {c->gather_stamp, c->d_gctr, c->d_pf_edits[0], c->d_pf_edits[1], c->d_gather_list, c->d_gather_dst};
     for (void* p : gdev) if (p) cudaFree(p);
     if (c->h_gctr) cudaFreeHost(c->h_gctr);
     if (c->h_pf_edits) cudaFreeHost(c->h_pf_edits);
@@ -184,6 +185,7 @@ int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
     }
     for (int i = 0; i < 8 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
     ok = ok && cudaEventCreate(&c->ev_gather0) == cudaSuccess && cudaEventCreate(&c->ev_gather1) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_pf, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaMallocHost((void**)&c->h_ctr, sizeof(DevCounters)) == cudaSuccess &&
          cudaMallocHost((void**)&c->h_bar, sizeof(GridBar)) == cudaSuccess;
     if (!ok) { cudaError_t le = cudaGetLastError(); release(c); return cuda_fail(nullptr, le, "context streams"); }
@@ -402,8 +404,12 @@ int scout_repair(scout_ctx* c, int problem, const scout_edge* edits, const uint8
     if (sched) sd = *sched;
     SCOUT_RC(apply_tuning(c, sd));
     const int64_t launch0 = c->nlaunch;
-    SCOUT_RC(batch_prologue(c, problem, edits, ops, m, st));
-    SCOUT_RC(gather_launch(c, c->merge_tail));   // the next batch's cold rows, during this repair
+    c->pf_use = sd.prefetched != 0;
+    const int prc = batch_prologue(c, problem, edits, ops, m, st);
+    c->pf_use = false;
+    SCOUT_RC(prc);
+    // the hinted next batch: its edits' copy (and, tiered, its cold rows' gather) during this repair
+    SCOUT_RC(prefetch_launch(c, c->merge_tail));
     const int* mode_dev = nullptr;
     const int variant = plain_variant(problem, sd);
     if (sd.policy == SCOUT_SCHED_LEARNED && sched_variants(problem) > 1)

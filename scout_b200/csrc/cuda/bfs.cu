@@ -417,7 +417,9 @@ __device__ bool full_bfs(const BfsParams& p, int mode, long long& bytes, int& ro
     return true;
 }
 
-__global__ void __launch_bounds__(BFS_THREADS) k_bfs(BfsParams p) {
+// At least four blocks per SM: the register budget this grants (64 per thread) holds the
+// kernel without spills (the unconstrained build spilled to local memory at 40 registers).
+__global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs(BfsParams p) {
     const int W = gwarp_count();
     const int wid = gwarp_id();
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;

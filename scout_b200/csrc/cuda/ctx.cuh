@@ -92,8 +92,14 @@ struct scout_ctx {
     // gather of the next batch's cold rows (tiered store; scout_prefetch, gather.cu)
     bool pf_pending = false;        // a hint waits for the next repair's merge
     int64_t pf_m = 0;
-    void* h_pf_edits = nullptr;  int64_t cap_h_pf_edits = 0;   // pinned copy of the hinted edits
-    scout_edge* d_pf_edits = nullptr;  int64_t cap_pf_edits = 0;
+    const scout_edge* pf_host = nullptr;   // where the hinted edits are read from (page-locked)
+    void* h_pf_edits = nullptr;  int64_t cap_h_pf_edits = 0;   // pinned copy of pageable hinted edits
+    scout_edge* d_pf_edits[2] = {nullptr, nullptr};  int64_t cap_pf_edits[2] = {0, 0};
+    int pf_slot = 0;                // slot of the latest copy of hinted edits
+    bool pf_ready = false;          // that slot holds (once ev_pf completes) a batch not yet used
+    int64_t pf_ready_m = 0;
+    bool pf_use = false;            // this call's edits are the hinted batch (scout_sched.prefetched)
+    cudaEvent_t ev_pf = nullptr;    // the hinted edits' copy is done (copy stream)
     int32_t* gather_stamp = nullptr;   // n: last gather that took the vertex's row
     uint32_t gather_tag = 0;
     void* d_gctr = nullptr;
@@ -285,9 +291,12 @@ int sched_variants(int problem);   // repair variants a problem has (BFS 3, CC 2
 int commit_gather(scout_ctx* c, int problem, const int32_t** pairs, int64_t* count);
 // persistent launch helper
 int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t smem);
-// gather.cu: the hinted next batch's cold rows into free HBM from `base` on a copy stream, after
-// the current merge; gather_finish waits for it (main stream and host) and moves the tail.
-int gather_launch(scout_ctx* c, long long base);
+// gather.cu: the hinted next batch's edits to the device and (tiered store) its cold rows into
+// free HBM from `base` on a copy stream, after the current merge is queued; gather_finish waits
+// for the gather (main stream and host) and moves the tail.
+int prefetch_launch(scout_ctx* c, long long base);
+// graph.cu: host copy into page-locked staging, over the host threads for large copies
+void stage_copy(void* dst, const void* src, size_t bytes);
 int gather_finish(scout_ctx* c, double* ms, int64_t* rows, int64_t* bytes);
 int gather_reserve(scout_ctx* c, int64_t max_edits);
 

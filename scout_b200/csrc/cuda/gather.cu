@@ -1,13 +1,15 @@
-// gather.cu -- per-batch gather of cold rows into HBM for the tiered store, overlapped with the
-// previous batch's repair (the fetch of batch K+1 while batch K repairs).
+// gather.cu -- the fetch of batch K+1 while batch K repairs: the next batch's edits are copied
+// to the device, and in the tiered store its cold rows are gathered into HBM, on a copy stream.
 //
 // The reference fetches the affected neighbourhoods of every batch from its mmap into pinned
 // staging and copies them to the device (scout_mis.cu:500-627, scout_bfs.cu:199-229), and only
 // its MIS engine prepares batch K+1 while batch K runs on the GPU (scout_mis.cu:855-912). Here
 // the graph lives in HBM except for the tiered store's cold rows, which sit in mapped
 // page-locked host memory and are read in place. scout_prefetch(next edits) makes the next
-// scout_repair call, once its own merge is done, gather the rows of the hinted edits'
-// endpoints that are still cold into free HBM on a copy stream, while its repair runs:
+// scout_repair call, once its own merge is queued, copy the hinted edits to the device on a
+// copy stream (a later scout_repair that declares them, scout_sched.prefetched, skips its own
+// upload) and, in the tiered store, gather the rows of their endpoints that are still cold
+// into free HBM, while its repair runs:
 //   k_gather_plan   one thread per endpoint: a cold row seen for the first time in this gather
 //                   (a stamp per vertex) takes space in the free HBM region by an atomic bump
 //                   (lengths rounded up to 4 entries, so every copy starts 16-byte aligned);
@@ -106,26 +108,35 @@ __global__ void __launch_bounds__(GATHER_THREADS) k_gather_copy(Row* __restrict_
     if (lane_id() == 0 && moved) atomicAdd(&gc->bytes, (unsigned long long)moved * 4);
 }
 
-// Launches the gather of the hinted edits on the copy stream after the main stream's merge
-// (ev_gather0 / ev_gather1 bracket it on that stream). base: first free HBM element after the
-// merge.
-int gather_launch(scout_ctx* c, long long base) {
+// After the current batch's merge has been queued on the main stream: the hinted next batch's
+// edits are copied to the device on the copy stream (ev_pf marks the end), and in the tiered
+// store its endpoints' cold rows are then gathered into HBM from `base` (ev_gather0 /
+// ev_gather1 bracket the copy and the gather). Both overlap the current batch's repair.
+int prefetch_launch(scout_ctx* c, long long base) {
     c->gather_active = false;
-    if (!c->tiered || !c->pf_pending || c->pf_m == 0) { c->pf_pending = false; return SCOUT_OK; }
+    if (!c->pf_pending || c->pf_m == 0) { c->pf_pending = false; return SCOUT_OK; }
     c->pf_pending = false;
     const int64_t m = c->pf_m;
-    const long long room = (long long)c->pool_cap - base - 4096;
-    if (room <= 0) return SCOUT_OK;
     SCOUT_RC(gather_reserve(c, m));
     cudaStream_t s = c->s_copy[1];
-    SCOUT_CU(c, cudaEventRecord(c->ev_copy[0], c->s_main));   // the merge is done
+    // two slots: the merge just queued may read the latest one (when this batch was the
+    // previous hint), so the new copy goes to the other, once the work queued so far is done
+    const int slot = 1 - c->pf_slot;
+    scout_edge* dst = c->d_pf_edits[slot];
+    SCOUT_CU(c, cudaEventRecord(c->ev_copy[0], c->s_main));
     SCOUT_CU(c, cudaStreamWaitEvent(s, c->ev_copy[0], 0));
-    SCOUT_CU(c, cudaEventRecord(c->ev_gather0, s));
+    if (c->tiered) SCOUT_CU(c, cudaEventRecord(c->ev_gather0, s));
+    SCOUT_CU(c, cudaMemcpyAsync(dst, c->pf_host, (size_t)m * sizeof(scout_edge), cudaMemcpyHostToDevice, s));
+    SCOUT_CU(c, cudaEventRecord(c->ev_pf, s));
+    c->pf_slot = slot;
+    c->pf_ready = true;
+    c->pf_ready_m = m;
+    const long long room = (long long)c->pool_cap - base - 4096;
+    if (!c->tiered || room <= 0) return SCOUT_OK;
     SCOUT_CU(c, cudaMemsetAsync(c->d_gctr, 0, sizeof(GatherCtr), s));
-    SCOUT_CU(c, cudaMemcpyAsync(c->d_pf_edits, c->h_pf_edits, (size_t)m * sizeof(scout_edge), cudaMemcpyHostToDevice, s));
     c->gather_tag = c->gather_tag + 1 == 0 ? 1 : c->gather_tag + 1;
     k_gather_plan<<<blocks_for(2 * m, GATHER_THREADS, c->sm_count), GATHER_THREADS, 0, s>>>(
-        c->row, (int32_t)c->n, c->d_pf_edits, m, (long long)c->pool_cap, c->gather_stamp, (int32_t)c->gather_tag, base, room,
+        c->row, (int32_t)c->n, dst, m, (long long)c->pool_cap, c->gather_stamp, (int32_t)c->gather_tag, base, room,
         c->d_gather_list, c->d_gather_dst, (GatherCtr*)c->d_gctr);
     // one block per SM: the copy is bound by the host link, and the repair's persistent kernel
     // (up to four 256-thread blocks per SM) must still fit beside it to run concurrently
@@ -140,9 +151,13 @@ int gather_launch(scout_ctx* c, long long base) {
     return SCOUT_OK;
 }
 
-// Buffers a gather of batches of up to max_edits edits needs (tiered store), allocated now.
+// Buffers a prefetch of batches of up to max_edits edits needs, allocated now: the device copy
+// of the hinted edits, and in the tiered store the gather's stamps, counters and lists.
 int gather_reserve(scout_ctx* c, int64_t max_edits) {
-    if (!c->tiered || max_edits <= 0) return SCOUT_OK;
+    if (max_edits <= 0) return SCOUT_OK;
+    for (int i = 0; i < 2; i++)
+        SCOUT_RC(dev_grow(c, &c->d_pf_edits[i], &c->cap_pf_edits[i], max_edits, "prefetched edits"));
+    if (!c->tiered) return SCOUT_OK;
     if (!c->gather_stamp) {
         SCOUT_RC(dev_alloc(c, (void**)&c->gather_stamp, (size_t)c->n * 4, "gather stamps"));
         SCOUT_CU(c, cudaMemsetAsync(c->gather_stamp, 0, (size_t)c->n * 4, c->s_main));
@@ -151,10 +166,8 @@ int gather_reserve(scout_ctx* c, int64_t max_edits) {
         SCOUT_RC(dev_alloc(c, (void**)&c->d_gctr, sizeof(GatherCtr), "gather counters"));
         SCOUT_CU(c, cudaMallocHost((void**)&c->h_gctr, sizeof(GatherCtr)));
     }
-    SCOUT_RC(dev_grow(c, &c->d_pf_edits, &c->cap_pf_edits, max_edits, "prefetched edits"));
     SCOUT_RC(dev_grow(c, &c->d_gather_list, &c->cap_gather_list, 2 * max_edits, "gather list"));
     SCOUT_RC(dev_grow(c, &c->d_gather_dst, &c->cap_gather_dst, 2 * max_edits, "gather destinations"));
-    SCOUT_RC(pin_grow(c, &c->h_pf_edits, &c->cap_h_pf_edits, max_edits * (int64_t)sizeof(scout_edge)));
     return SCOUT_OK;
 }
 
@@ -189,11 +202,21 @@ extern "C" int scout_prefetch(scout_ctx* c, const scout_edge* next, int64_t m) {
     if (!c || m < 0 || (m > 0 && !next)) return c ? c->fail(SCOUT_E_INVALID, "bad arguments") : SCOUT_E_INVALID;
     c->pf_pending = false;
     c->pf_m = 0;
-    if (!c->tiered || m == 0) return SCOUT_OK;   // every row is in HBM: nothing to gather
-    // the copy stream may still read the previous hint's edits
+    // the copy stream may still read the previous hint's edits (from the staging buffer
+    // overwritten below) or gather its rows; a copy already made stays usable
     if (c->gather_active) SCOUT_CU(c, cudaEventSynchronize(c->ev_gather1));
-    SCOUT_RC(pin_grow(c, &c->h_pf_edits, &c->cap_h_pf_edits, m * (int64_t)sizeof(scout_edge)));
-    std::memcpy(c->h_pf_edits, next, (size_t)m * sizeof(scout_edge));
+    if (c->pf_ready) SCOUT_CU(c, cudaEventSynchronize(c->ev_pf));
+    if (m == 0) return SCOUT_OK;
+    cudaPointerAttributes at;
+    const bool pinned = cudaPointerGetAttributes(&at, next) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    if (!pinned) cudaGetLastError();
+    if (pinned) {
+        c->pf_host = next;   // read in place by the copy: unchanged until the repair that uses it
+    } else {
+        SCOUT_RC(pin_grow(c, &c->h_pf_edits, &c->cap_h_pf_edits, m * (int64_t)sizeof(scout_edge)));
+        stage_copy(c->h_pf_edits, next, (size_t)m * sizeof(scout_edge));
+        c->pf_host = (const scout_edge*)c->h_pf_edits;
+    }
     c->pf_m = m;
     c->pf_pending = true;
     return SCOUT_OK;

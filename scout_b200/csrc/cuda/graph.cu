@@ -24,8 +24,9 @@
 //   k_plan_place      per insertion: its final slot in the new row; per matched deletion: the
 //                     old entry's tombstone (sign bit); per row: the new descriptor
 //   k_merge_small     survivors of short rows, balanced groups of ~UNIT entries per warp
-//   k_merge_slices    survivors of long rows, one warp per slice of SLICE entries, so a hub
+//   k_merge_slices    survivors of longer rows, one warp per slice of SLICE entries, so a hub
 //                     row is spread over many warps
+//   k_merge_long_inplace  rows longer than a slice that only lose entries, a block per row
 #include "ctx.cuh"
 
 #include <algorithm>
@@ -33,15 +34,17 @@
 
 namespace scout {
 
-constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the long-row merge
-constexpr int SMALL_LEN = 2048;      // rows up to this length go to the short-row merge
+constexpr int SLICE = 4096;          // old-row entries streamed by one warp in the slice merge
+constexpr int SMALL_LEN = 128;       // rows up to this length go to the short-row merge
 
 // A row whose half-edits are all deletions is rewritten in place: its survivors only move
 // towards the row start, it keeps its start and capacity, and it takes no pool space (short
-// rows in the short-row merge, longer ones by one block each in k_merge_long_inplace).
-__host__ __device__ __forceinline__ bool in_place_row(long long insertions, int old_len) {
-    (void)old_len;
-    return insertions == 0;
+// rows in the short-row merge, rows of one slice by their warp in the slice merge). A longer
+// one is compacted in place by one block (k_merge_long_inplace: its slices would overlap) only
+// when `long_in_place` is set, in the tiered store, whose HBM room is scarce; in the all-HBM
+// store it is rewritten at the pool tail by the slice merge, spread over many warps.
+__host__ __device__ __forceinline__ bool in_place_row(long long insertions, int old_len, bool long_in_place) {
+    return insertions == 0 && (old_len <= SLICE || long_in_place);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -231,11 +234,12 @@ __device__ __forceinline__ long long warp_lower_bound(const int64_t* a, long lon
 
 // Per affected row: its descriptor before the batch and the space of its new row (old length
 // + insertions: slots of matched deletions stay unused until the next compaction). Rows up
-// to SMALL_LEN entries go to the short-row merge, longer ones are cut into merge slices.
+// to SMALL_LEN entries go to the short-row merge, longer ones are cut into merge slices
+// (rows past one slice that only lose entries go to the in-place block merge instead).
 __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict__ ctr, const int32_t* __restrict__ aff,
                             const int64_t* __restrict__ seg, Row* __restrict__ old_row, int64_t* __restrict__ alloc,
                             int32_t* __restrict__ small, int64_t* __restrict__ small_len, int64_t* __restrict__ slices,
-                            int64_t slice_cap, int32_t* __restrict__ longs) {
+                            int64_t slice_cap, int32_t* __restrict__ longs, bool long_in_place) {
     const int A = ctr->n_aff;
     const int T = gridDim.x * blockDim.x;
     for (int b = (int)(blockIdx.x * blockDim.x + threadIdx.x) - (int)lane_id(); b < A; b += T) {
@@ -247,10 +251,10 @@ __global__ void k_row_alloc(const Row* __restrict__ row, DevCounters* __restrict
             const long long b0 = seg[3 * (int64_t)a], sp = seg[3 * (int64_t)a + 1];
             const Row r = row[aff[a]];
             old_row[a] = r;
-            const bool ip = in_place_row(sp - b0, r.len);
+            const bool ip = in_place_row(sp - b0, r.len, long_in_place);
             alloc[a] = ip ? 0 : (long long)r.len + (sp - b0);
             sm = r.len <= SMALL_LEN;
-            lip = !sm && ip;   // a long row that only loses entries: compacted in place by one block
+            lip = ip && r.len > SLICE;   // longer than a slice, compacted in place: one block
             ns = sm || lip ? 0 : (r.len + SLICE - 1) / SLICE;
         }
         const int lat = warp_append(lip, &ctr->n_large);
@@ -319,7 +323,7 @@ __global__ void k_plan_place(int32_t* __restrict__ pool, Row* __restrict__ row, 
                              int B, DevCounters* __restrict__ ctr, const int32_t* __restrict__ slot,
                              const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
                              const int64_t* __restrict__ off, long long tail, const long long* __restrict__ dpos,
-                             const long long* __restrict__ E) {
+                             const long long* __restrict__ E, bool long_in_place) {
     const long long nh = ctr->n_half;
     long long nnz_delta = 0, bytes = 0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nh; k += (long long)gridDim.x * blockDim.x) {
@@ -342,7 +346,7 @@ __global__ void k_plan_place(int32_t* __restrict__ pool, Row* __restrict__ row, 
         if (k == b0) {
             const long long p = sp - b0, q = e0 - sp;
             const long long nl = (long long)r.len + p - (E[e0] - E[sp]);
-            row[u] = in_place_row(p, r.len) ? Row{r.start, (int)nl, r.cap}
+            row[u] = in_place_row(p, r.len, long_in_place) ? Row{r.start, (int)nl, r.cap}
                                             : Row{tail + off[a], (int)nl, (int)(r.len + p)};
             nnz_delta += nl - r.len;
             bytes += 4 * (r.len + nl) + 8 * (p + q) + 16;
@@ -396,7 +400,7 @@ __global__ void __launch_bounds__(MERGE_THREADS) k_merge_small(
                 len = r.len;
                 ib = seg[3 * (int64_t)a];
                 p = (int)(seg[3 * (int64_t)a + 1] - ib);
-                ob = in_place_row(p, len) ? st : tail + off[a];
+                ob = in_place_row(p, len, false) ? st : tail + off[a];   // short: the flag is moot
             }
             s_cnt[w][lane] = 0;
             const int pin = warp_incl_scan_i(p);
@@ -525,7 +529,10 @@ __global__ void __launch_bounds__(LIP_THREADS) k_merge_long_inplace(int32_t* __r
     }
 }
 
-// Long rows: one warp per slice of SLICE old-row entries. The survivors before the slice are
+// Rows past SMALL_LEN: one warp per slice of SLICE old-row entries (most rows a batch touches
+// in a scale-free graph are its hubs, so this merge carries most of the bytes, with a few
+// instructions per entry: a ballot, a population count, and a search of the insertions only
+// where they fall inside a chunk's value range). The survivors before the slice are
 // its start minus the matched deletions before it (one search in the non-decreasing dpos);
 // survivor x lands at (#survivors before it) + (#insertions < x), the insertion count
 // searched only inside the range spanned by the chunk's values.
@@ -541,6 +548,7 @@ constexpr int MS_WARPS = 8;
 constexpr int MS_THREADS = MS_WARPS * WARP;
 constexpr int MS_CH = 512;                 // entries per staged chunk
 constexpr int MS_BUF = MS_CH + 8;          // buffer: chunk + 16-byte alignment slack on both ends
+constexpr int MS_ISTAGE = 256;             // insertion keys of one merge step staged per warp
 constexpr long long MBAR_SPIN_LIMIT = 1ll << 24;
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -572,11 +580,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
     return false;
 }
 
+// First index i in [from, p] with I[i] >= t (I ascending), the warp reading 32 keys per step
+// forward from `from`; every lane calls it and gets the same answer.
+__device__ __forceinline__ long long ins_advance(const KeySpan& I, long long p, long long from, int32_t t) {
+    for (long long i = from; i < p; i += WARP) {
+        const long long j = i + lane_id();
+        const unsigned m = __ballot_sync(0xffffffffu, j < p && I[j] < t);   // a prefix of the lanes
+        const int k = __popc(m);
+        if (k < WARP) return i + k;
+    }
+    return p;
+}
+
 // Merges old-row entries [b, e) (absolute pool indices) read through `get`, updating the running
-// survivor count; every lane calls it.
+// survivor count; every lane calls it. Survivor x lands at run + (survivors before it in its
+// step) + (insertions < x). The insertions below the step's smallest value are `cur`, which
+// only moves forward along the row (the old entries are ascending): each step advances it to
+// its value range [xmin, xmax) with coalesced reads of the insertion keys, stages the keys of
+// that range in shared memory (s_ins, MS_ISTAGE entries) and searches them there.
 template <typename Get>
 __device__ __forceinline__ void merge_span(long long b, long long e, Get get, int32_t* out, long long& run,
-                                           const KeySpan& I, long long p, unsigned lt) {
+                                           const KeySpan& I, long long p, long long& cur, int32_t* s_ins,
+                                           unsigned lt) {
     constexpr int U = 4;
     for (long long base = b; base < e; base += U * WARP) {
         int32_t x[U];
@@ -585,20 +610,24 @@ __device__ __forceinline__ void merge_span(long long b, long long e, Get get, in
             const long long i = base + u * WARP + lane_id();
             x[u] = i < e ? get(i) : -1;
         }
-        long long cl = 0, ch = 0;
-        if (p > 0) {
+        long long cl = cur, nin = 0;
+        if (cur < p) {
             int xmin = INT32_MAX, xmax = -1;
 #pragma unroll
             for (int u = 0; u < U; u++)
                 if (x[u] >= 0) { xmin = min(xmin, x[u]); xmax = max(xmax, x[u]); }
             xmin = __reduce_min_sync(0xffffffffu, xmin);
             xmax = __reduce_max_sync(0xffffffffu, xmax);
-            if (xmax >= 0 && lane_id() == 0) {
-                cl = lb_span(I, p, xmin);
-                ch = cl + lb_span(KeySpan{I.k + cl, I.B}, p - cl, xmax);
+            if (xmax >= 0) {
+                cl = ins_advance(I, p, cur, xmin);
+                const long long ch = ins_advance(I, p, cl, xmax);
+                nin = ch - cl;
+                cur = ch;
+                if (nin > 0 && nin <= MS_ISTAGE) {
+                    for (long long j = lane_id(); j < nin; j += WARP) s_ins[j] = I[cl + j];
+                    __syncwarp();
+                }
             }
-            cl = __shfl_sync(0xffffffffu, cl, 0);
-            ch = __shfl_sync(0xffffffffu, ch, 0);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -606,11 +635,20 @@ __device__ __forceinline__ void merge_span(long long b, long long e, Get get, in
             const unsigned m = __ballot_sync(0xffffffffu, surv);
             if (surv) {
                 long long lbI = cl;
-                if (ch > cl) lbI = cl + lb_span(KeySpan{I.k + cl, I.B}, ch - cl, x[u]);
+                if (nin > 0) {
+                    if (nin <= MS_ISTAGE) {
+                        int lo = 0, hi = (int)nin;
+                        while (lo < hi) { const int mid = (lo + hi) >> 1; if (s_ins[mid] < x[u]) lo = mid + 1; else hi = mid; }
+                        lbI += lo;
+                    } else {
+                        lbI += lb_span(KeySpan{I.k + cl, I.B}, nin, x[u]);
+                    }
+                }
                 out[run + __popc(m & lt) + lbI] = x[u];
             }
             run += __popc(m);
         }
+        __syncwarp();   // s_ins is read before the next step stages another range
     }
 }
 
@@ -618,9 +656,11 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
         int32_t* __restrict__ pool, long long pool_cap, const unsigned long long* __restrict__ keys, int B,
         DevCounters* __restrict__ ctr, const int64_t* __restrict__ seg, const Row* __restrict__ old_row,
         const int64_t* __restrict__ off, long long tail, const long long* __restrict__ E,
-        const long long* __restrict__ dpos, const int64_t* __restrict__ slices, int64_t slice_cap) {
+        const long long* __restrict__ dpos, const int64_t* __restrict__ slices, int64_t slice_cap,
+        bool long_in_place) {
     __shared__ __align__(16) int32_t s_buf[MS_WARPS][2][MS_BUF];
     __shared__ __align__(8) uint64_t s_bar[MS_WARPS][2];
+    __shared__ int32_t s_ins[MS_WARPS][MS_ISTAGE];
     const int w = threadIdx.x / WARP;
     const unsigned lt = (1u << lane_id()) - 1;
     if (lane_id() == 0) {
@@ -646,12 +686,20 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
             md = E[sp + lo] - E[sp];
         }
         long long run = s0 - __shfl_sync(0xffffffffu, md, 0);
-        int32_t* out = pool + tail + off[a];
+        // a row compacted in place is one slice here: every survivor lands at or before its old
+        // position, which its warp has already read
+        int32_t* out = pool + (in_place_row(p, r.len, long_in_place) ? r.start : tail + off[a]);
         const KeySpan I{keys + b0, B};
         const long long abs0 = r.start + s0, abs1 = r.start + s1;   // pool indices of the slice
+        // insertions below the slice's first value (tombstones keep the value under the sign bit)
+        long long cur = 0;
+        if (s0 > 0 && p > 0) {
+            if (lane_id() == 0) cur = lb_span(I, p, unmark(pool[abs0]));
+            cur = __shfl_sync(0xffffffffu, cur, 0);
+        }
         const bool staged = r.start >= 0 && ((abs1 + 3) & ~3LL) <= pool_cap;
         if (!staged) {
-            merge_span(abs0, abs1, [&](long long i) { return pool[i]; }, out, run, I, p, lt);
+            merge_span(abs0, abs1, [&](long long i) { return pool[i]; }, out, run, I, p, cur, s_ins[w], lt);
             continue;
         }
         const int nch = (int)((s1 - s0 + MS_CH - 1) / MS_CH);
@@ -676,7 +724,7 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
             phase[bsel] ^= 1u;
             const long long lo = abs0 + (long long)k * MS_CH, hi = min(abs1, lo + MS_CH);
             const int32_t* sb = s_buf[w][bsel] - (lo & ~3LL);   // indexed by absolute pool index
-            merge_span(lo, hi, [&](long long i) { return sb[i]; }, out, run, I, p, lt);
+            merge_span(lo, hi, [&](long long i) { return sb[i]; }, out, run, I, p, cur, s_ins[w], lt);
             __syncwarp();   // every lane is done with this buffer before it is refilled
             if (k + 2 < nch && lane_id() == 0) {
                 fence_proxy_async_smem();   // the warp's reads of the buffer precede the copy's writes
@@ -1144,7 +1192,7 @@ static bool is_pinned(const void* p) {
 }
 
 // Host memcpy into the pinned staging buffer, split over the host threads for large batches.
-static void stage_copy(void* dst, const void* src, size_t bytes) {
+void stage_copy(void* dst, const void* src, size_t bytes) {
     constexpr size_t PART = (size_t)1 << 20;
     if (bytes < 4 * PART) {
         std::memcpy(dst, src, bytes);
@@ -1160,7 +1208,19 @@ static void stage_copy(void* dst, const void* src, size_t bytes) {
 
 // Edits in pinned host memory are copied to the device directly; pageable ones go through the
 // context's pinned staging buffer.
-static int upload_edits(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m) {
+// Edits hinted by scout_prefetch and declared by this call are already on their way to the
+// device (copy stream, ev_pf): the main stream waits for that copy and reads them there.
+static int upload_edits(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int64_t m,
+                        const scout_edge** d_src) {
+    const bool hinted = c->pf_use && c->pf_ready && c->pf_ready_m == m && !ops;
+    c->pf_use = false;
+    if (c->pf_ready) c->pf_ready = false;   // consumed now, or stale (the next hint replaces it)
+    if (hinted) {
+        SCOUT_CU(c, cudaStreamWaitEvent(c->s_main, c->ev_pf, 0));
+        *d_src = c->d_pf_edits[c->pf_slot];
+        return SCOUT_OK;
+    }
+    *d_src = c->d_edits;
     const size_t eb = (size_t)m * sizeof(scout_edge);
     const bool pe = is_pinned(edits), po = !ops || is_pinned(ops);
     if (!pe || !po) {
@@ -1204,10 +1264,11 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
         SCOUT_CU(c, cudaEventRecord(c->ev_t[3], c->s_main));
         return SCOUT_OK;
     }
-    SCOUT_RC(upload_edits(c, edits, ops, m));
+    const scout_edge* d_src = nullptr;
+    SCOUT_RC(upload_edits(c, edits, ops, m, &d_src));
     SCOUT_CU(c, cudaEventRecord(c->ev_t[3], c->s_main));
     DGraph g = dgraph(c);
-    k_classify<<<blocks_for(m, 256), 256, 0, c->s_main>>>(g, c->d_edits, ops ? c->d_ops : nullptr, m, B, c->d_keys,
+    k_classify<<<blocks_for(m, 256), 256, 0, c->s_main>>>(g, d_src, ops ? c->d_ops : nullptr, m, B, c->d_keys,
                                                          c->d_eflag, c->d_ctr, 1);
     SCOUT_LAUNCH(c, "k_classify");
     c->nlaunch += 1;
@@ -1232,7 +1293,7 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
         k_row_alloc<<<blocks_for(Amax, 256), 256, 0, c->s_main>>>(c->row, c->d_ctr, c->d_aff, c->d_aff_seg,
                                                                   c->d_old_row, c->d_aff_len, c->d_aff_small,
                                                                   c->d_small_off, c->d_slices, c->cap_slices,
-                                                                  c->d_aff_long);
+                                                                  c->d_aff_long, c->tiered);
         SCOUT_LAUNCH(c, "k_row_alloc");
         c->nlaunch += 1;
         if (split) {
@@ -1315,18 +1376,24 @@ int graph_update(scout_ctx* c, const scout_edge* edits, const uint8_t* ops, int6
     SCOUT_RC(scan_i64(c, (int64_t*)E, H + 1, nullptr));
     k_plan_place<<<blocks_for(H, 256), 256, 0, c->s_main>>>(c->pool, c->row, sorted, B, c->d_ctr, c->aux_w,
                                                             c->d_aff_seg, c->d_old_row, c->d_aff_len,
-                                                            dest, dpos, E);
+                                                            dest, dpos, E, c->tiered);
     SCOUT_LAUNCH(c, "k_plan_place");
     SCOUT_RC(scan_i64(c, c->d_small_off, Amax + 1, nullptr));
+    // the row merges loop over their work lists: a grid of at most four blocks per SM
     const int64_t groups = std::min<int64_t>(c->nnz, Amax * (int64_t)SMALL_LEN) / UNIT + 1;
-    k_merge_small<<<blocks_for(groups * WARP, MERGE_THREADS), MERGE_THREADS, 0, c->s_main>>>(
+    const int res4 = 4 * c->sm_count;
+    k_merge_small<<<std::min(blocks_for(groups * WARP, MERGE_THREADS), res4), MERGE_THREADS, 0, c->s_main>>>(
         c->pool, sorted, B, c->d_ctr, c->d_aff_seg, c->d_old_row, c->d_aff_len, dest, c->d_aff_small,
         c->d_small_off);
     k_merge_long_inplace<<<(unsigned)std::min<int64_t>(std::max<int64_t>(1, Amax), 8 * (int64_t)c->sm_count),
                            LIP_THREADS, 0, c->s_main>>>(c->pool, c->d_ctr, c->d_aff_long, c->d_old_row);
-    k_merge_slices<<<blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + 1024) * WARP, MS_THREADS), MS_THREADS,
+    k_merge_slices<<<std::min(blocks_for(std::min<int64_t>(c->cap_slices, c->nnz / SLICE + Amax + 1024) * WARP,
+                                         MS_THREADS),
+                              res4),
+                     MS_THREADS,
                      0, c->s_main>>>(c->pool, (long long)c->pool_cap, sorted, B, c->d_ctr, c->d_aff_seg,
-                                     c->d_old_row, c->d_aff_len, dest, E, dpos, c->d_slices, c->cap_slices);
+                                     c->d_old_row, c->d_aff_len, dest, E, dpos, c->d_slices, c->cap_slices,
+                                     c->tiered);
     SCOUT_LAUNCH(c, "merge");
     c->nlaunch += 6;
     return SCOUT_OK;
@@ -1346,10 +1413,15 @@ int scout_graph_reserve(scout_ctx* c, int64_t n, int64_t nnz) {
     c->n = n;
     SCOUT_RC(dev_alloc(c, (void**)&c->row, (size_t)n * sizeof(Row), "row table"));
     SCOUT_CU(c, cudaMemsetAsync(c->row, 0, (size_t)n * sizeof(Row), c->s_main));
-    // Room for several batches of rewritten rows between compactions (HBM is plentiful; a
-    // budget that cannot hold four times the graph falls back to twice).
-    c->pool_cap = 4 * nnz + (1 << 26);
-    if ((uint64_t)c->pool_cap * 4 * 2 + c->held > c->budget) c->pool_cap = 2 * nnz + (1 << 22);
+    // Room for several batches of rewritten rows between compactions: a compaction copies every
+    // live row whatever the garbage, so the larger the pool, the rarer they are. HBM is
+    // plentiful (the pool and its compaction spare at eight times a 128 M-entry graph are
+    // 8.6 GB); a budget that cannot hold that falls back to four, then two times the graph.
+    const int64_t mult[3] = {8, 4, 2};
+    for (int i = 0; i < 3; i++) {
+        c->pool_cap = mult[i] * nnz + (i < 2 ? (1 << 26) : (1 << 22));
+        if ((uint64_t)c->pool_cap * 4 * 2 + c->held <= c->budget) break;
+    }
     SCOUT_RC(dev_alloc(c, (void**)&c->pool, (size_t)c->pool_cap * sizeof(int32_t), "element pool"));
     c->tail = 0;
     c->nnz = 0;

@@ -315,35 +315,50 @@ __global__ void k_scan_apply(T* __restrict__ a, int64_t n, const int64_t* __rest
     }
 }
 
-// Arrays of up to SCAN_ONE_MAX entries are scanned by one 1024-thread block in one launch (each
-// thread a contiguous run of at most 64 entries); longer ones by the three-launch tile scan.
+// Arrays of up to SCAN_ONE_MAX entries are scanned by one 1024-thread block in one launch, in
+// steps of SCAN_ONE_STEP entries: each thread loads SCAN_ONE_IPT consecutive entries (a warp
+// reads one contiguous 2 KB span), the block scans the thread sums, and a running carry links
+// the steps. Longer arrays take the three-launch tile scan.
 constexpr int64_t SCAN_ONE_MAX = 1 << 16;
 constexpr int SCAN_ONE_THREADS = 1024;
+constexpr int SCAN_ONE_IPT = 8;
+constexpr int SCAN_ONE_STEP = SCAN_ONE_THREADS * SCAN_ONE_IPT;
 
 template <typename T>
 __global__ void __launch_bounds__(SCAN_ONE_THREADS) k_scan_one(T* __restrict__ a, int64_t n, int64_t* __restrict__ d_total) {
     __shared__ long long ws[SCAN_ONE_THREADS / WARP];
+    __shared__ long long s_step;
     const int t = threadIdx.x, w = t / WARP, lane = t & (WARP - 1);
-    const int64_t per = (n + SCAN_ONE_THREADS - 1) / SCAN_ONE_THREADS;
-    const int64_t lo = (int64_t)t * per, hi = lo + per < n ? lo + per : n;
-    long long s = 0;
-    for (int64_t i = lo; i < hi; i++) s += (long long)a[i];
-    const long long inc = warp_incl_scan(s);
-    if (lane == WARP - 1) ws[w] = inc;
-    __syncthreads();
-    if (w == 0) {
-        const long long v = ws[lane];
-        const long long vi = warp_incl_scan(v);
-        ws[lane] = vi - v;
-        if (lane == WARP - 1 && d_total) *d_total = vi;
+    long long carry = 0;
+    for (int64_t base = 0; base < n; base += SCAN_ONE_STEP) {
+        const int64_t i0 = base + (int64_t)t * SCAN_ONE_IPT;
+        long long x[SCAN_ONE_IPT];
+        long long s = 0;
+#pragma unroll
+        for (int k = 0; k < SCAN_ONE_IPT; k++) {
+            x[k] = i0 + k < n ? (long long)a[i0 + k] : 0;
+            s += x[k];
+        }
+        const long long inc = warp_incl_scan(s);
+        if (lane == WARP - 1) ws[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            const long long v = ws[lane];
+            const long long vi = warp_incl_scan(v);
+            ws[lane] = vi - v;
+            if (lane == WARP - 1) s_step = vi;
+        }
+        __syncthreads();
+        long long run = carry + ws[w] + inc - s;
+#pragma unroll
+        for (int k = 0; k < SCAN_ONE_IPT; k++) {
+            if (i0 + k < n) a[i0 + k] = (T)run;
+            run += x[k];
+        }
+        carry += s_step;
+        __syncthreads();   // ws and s_step are read before the next step writes them
     }
-    __syncthreads();
-    long long run = ws[w] + inc - s;
-    for (int64_t i = lo; i < hi; i++) {
-        const long long x = (long long)a[i];
-        a[i] = (T)run;
-        run += x;
-    }
+    if (t == 0 && d_total) *d_total = carry;
 }
 
 template <typename T>
@@ -419,7 +434,9 @@ int sort_keys(scout_ctx* c, unsigned long long* keys, unsigned long long* alt, i
     unsigned int* ctl = c->d_sort_hist;
     unsigned long long* lb = (unsigned long long*)(ctl + OS_CTRL_WORDS);
     SCOUT_CU(c, cudaMemsetAsync(ctl, 0, (size_t)(OS_DONE + 1) * 4, c->s_main));
-    const int hb = (int)std::min<int64_t>((n + OS_TILE - 1) / OS_TILE, 4 * (int64_t)c->sm_count);
+    // a block per 1024 keys (at most four per SM): the digit histograms of skewed keys (hub
+    // vertices) collide in shared memory, so fewer keys per block means shorter atomic queues
+    const int hb = (int)std::min<int64_t>((n + 1023) / 1024, 4 * (int64_t)c->sm_count);
     k_os_hist<<<hb, OS_THREADS, 0, c->s_main>>>(keys, n, passes, ctl);
     SCOUT_LAUNCH(c, "k_os_hist");
     c->nlaunch += 1;

@@ -207,11 +207,17 @@ class Context:
 
     # ---- repair -----------------------------------------------------------------------
     def repair(self, problem, edges, ops=None, sched: Optional[dict] = None) -> dict:
+        # the batch hinted by the last prefetch(): its device copy is already on the way
+        pf = getattr(self, "_pf", None)
+        hinted = pf is not None and edges is pf and ops is None
+        self._pf = None
         e = as_edges(edges)
         st = ScoutBatchStats()
         sd = ScoutSched()
         for k, v in (sched or {}).items():
             setattr(sd, k, v)
+        if hinted:
+            sd.prefetched = 1
         op = None
         if ops is not None:
             ops = np.ascontiguousarray(ops, dtype=np.uint8)
@@ -220,10 +226,15 @@ class Context:
         return st.as_dict()
 
     def prefetch(self, next_edges) -> None:
-        """Hint the edits of the batch after the next repair (tiered store: its cold rows are
-        gathered into HBM while that repair runs)."""
+        """Hint the edits of the batch after the next repair: that repair copies them to the
+        device while it runs (and, tiered store, gathers their cold rows into HBM), and a later
+        repair() given the same object uses the copy. A page-locked array (pinned_copy) is read
+        in place and must stay unchanged until then."""
         e = as_edges(next_edges)
         self._c(LIB.scout_prefetch(self._h, _pedge(e), len(e)))
+        # a converted temporary was copied by the call; only the caller's own array, passed to
+        # repair() unchanged, is declared as the hinted batch
+        self._pf = next_edges if e is next_edges else None
 
     def repair_probe(self, problem, edges, ops=None, sched: Optional[dict] = None):
         """One batch, every repair variant timed from the same pre-repair state (results must
