@@ -25,6 +25,7 @@
 namespace scout {
 
 constexpr int BFS_THREADS = 256;
+constexpr int PSCAN = 4;   // row entries per lane and step in the seed scan
 
 struct BfsParams {
     DGraph g;
@@ -88,6 +89,33 @@ __device__ __forceinline__ void push_vertex(const BfsParams& p, bool pred, int32
     for (int k = 0; k < nit; k++) {
         long long pos = start + k;
         if (pos < p.qcap) p.q[qi][pos] = ((unsigned long long)k << 32) | (uint32_t)y;
+        else atomicExch(&p.ctr->overflow, 1);
+    }
+}
+
+// push_vertex (chunked, no touch list) of two vertices per lane at once: the dedupe atomics and
+// row-length loads of both are in flight together, and one atomicAdd reserves both's items.
+__device__ __forceinline__ void push_vertex2(const BfsParams& p, bool pa, int32_t ya, bool pb, int32_t yb, int qi,
+                                             uint32_t tag) {
+    bool fa = false, fb = false;
+    if (pa) fa = atomicExch(&p.st_q[ya], tag) != tag;
+    if (pb) fb = atomicExch(&p.st_q[yb], tag) != tag;   // ya == yb: only the first push counts
+    int na = 0, nb = 0;
+    if (fa) na = max(1, (p.g.row[ya].len + p.chunk - 1) >> p.chunk_log2);
+    if (fb) nb = max(1, (p.g.row[yb].len + p.chunk - 1) >> p.chunk_log2);
+    const int nit = na + nb;
+    const int incl = warp_incl_scan_i(nit);
+    const int tot = __shfl_sync(0xffffffffu, incl, WARP - 1);
+    if (tot == 0) return;
+    int base = 0;
+    if (lane_id() == WARP - 1) base = atomicAdd(&p.ctr->q_count[qi], tot);
+    base = __shfl_sync(0xffffffffu, base, WARP - 1);
+    const long long start = (long long)base + incl - nit;
+    for (int k = 0; k < nit; k++) {
+        const long long pos = start + k;
+        const int32_t v = k < na ? ya : yb;
+        const int kk = k < na ? k : k - na;
+        if (pos < p.qcap) p.q[qi][pos] = ((unsigned long long)kk << 32) | (uint32_t)v;
         else atomicExch(&p.ctr->overflow, 1);
     }
 }
@@ -454,23 +482,28 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs(BfsParams p) {
         // candidate pushes its children, so a hub's row is spread over many warps.
         const int nh = ld_volatile(&p.ctr->n_half);
         tag++;
-        for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
-            int64_t k = b + lane_id();
-            bool cand = false;
-            int32_t y = 0;
-            if (k < nh) {
-                unsigned long long key = p.hkeys[k];
-                int op = (int)((key >> p.B) & 1ull);
-                int32_t x = (int32_t)(key >> (p.B + 1));
-                y = (int32_t)(key & ((1ull << p.B) - 1));
-                if (op == 1) {
-                    int lx = ld_level(p.level + x), ly = ld_level(p.level + y);
-                    cand = lx >= 0 && ly == lx + 1;
+        // two half-edits per thread and step (k and k + T): their loads overlap, and both
+        // candidates go out in one warp-collective push
+        for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += 2 * T) {
+            bool cand[2] = {false, false};
+            int32_t y[2] = {0, 0};
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int64_t k = b + h * T + lane_id();
+                if (k < nh) {
+                    const unsigned long long key = p.hkeys[k];
+                    const int op = (int)((key >> p.B) & 1ull);
+                    const int32_t x = (int32_t)(key >> (p.B + 1));
+                    y[h] = (int32_t)(key & ((1ull << p.B) - 1));
+                    if (op == 1) {
+                        const int lx = ld_level(p.level + x), ly = ld_level(p.level + y[h]);
+                        cand[h] = lx >= 0 && ly == lx + 1;
+                    }
                 }
             }
-            const unsigned mc = __ballot_sync(0xffffffffu, cand);   // tree-edge deletions
-            if (lane_id() == 0 && mc) atomicAdd(&p.ctr->del_eff, __popc(mc));
-            push_vertex(p, cand, y, 0, tag, true, false);
+            const int nc = __popc(__ballot_sync(0xffffffffu, cand[0])) + __popc(__ballot_sync(0xffffffffu, cand[1]));
+            if (lane_id() == 0 && nc) atomicAdd(&p.ctr->del_eff, nc);   // tree-edge deletions
+            push_vertex2(p, cand[0], y[0], cand[1], y[1], 0, tag);
         }
         if (!grid_sync(p.bar, 2)) return;
         cur = 0;
@@ -480,14 +513,38 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs(BfsParams p) {
             const int nxt = (cur + 1) % 3, zer = (cur + 2) % 3;
             if (leader) p.ctr->q_count[zer] = 0;
             tag++;
+            // Software pipeline over the warp's candidates: the queue item two candidates ahead,
+            // and the row, level and invalidation mark of the next one, are loaded while the
+            // current one is checked. None of them changes during this pass: levels are fixed in
+            // this phase, and a single-chunk candidate is queued once per round and invalidated
+            // only by its own warp (a long one's mark is set after the barrier below).
+            unsigned long long it_n = wid < cnt ? p.q[cur][wid] : 0ull;
+            Row r_n{0, 0, 0};
+            int lc_n = 0, si_n = 0;
+            if (wid < cnt) {
+                const int32_t cn = (int32_t)(it_n & 0xffffffffu);
+                r_n = p.g.row[cn];
+                lc_n = ld_level(p.level + cn);
+                si_n = ld_volatile(p.st_inval + cn);
+            }
+            unsigned long long it_nn = wid + W < cnt ? p.q[cur][wid + W] : 0ull;
             for (int i = wid; i < cnt; i += W) {
-                const unsigned long long item = p.q[cur][i];
+                const unsigned long long item = it_n;
+                const Row r = r_n;
+                const int lc = lc_n;
+                const int si = si_n;
+                it_n = it_nn;
+                if (i + W < cnt) {   // the next candidate's item arrived during this one's wait
+                    const int32_t cn = (int32_t)(it_n & 0xffffffffu);
+                    r_n = p.g.row[cn];
+                    lc_n = ld_level(p.level + cn);
+                    si_n = ld_volatile(p.st_inval + cn);
+                }
+                it_nn = (long long)i + 2 * W < cnt ? p.q[cur][i + 2 * W] : 0ull;
                 const int32_t c = (int32_t)(item & 0xffffffffu);
                 const int chunk = (int)(item >> 32);
-                const Row r = p.g.row[c];
                 const bool big = r.len > p.chunk;
-                const int lc = ld_level(p.level + c);
-                if (c == p.source || lc <= 0 || ld_volatile(p.st_inval + c) == p.epoch) {
+                if (c == p.source || lc <= 0 || si == p.epoch) {
                     if (big && lane_id() == 0) p.found[c] = (int32_t)tag;   // nothing to decide
                     continue;
                 }
@@ -495,15 +552,17 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs(BfsParams p) {
                 const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
                 const int32_t* rw = p.g.pool + r.start + c0;
                 bool found = false;
+                // 32 entries per step: most candidates keep a parent early in the row, and wider
+                // steps (measured with four entries per lane) only add random level reads
                 for (int b0 = 0; b0 < clen && !found; b0 += WARP) {
-                    int k = b0 + (int)lane_id();
+                    const int k = b0 + (int)lane_id();
                     bool ok = false;
                     if (k < clen) {
-                        int32_t w = rw[k];
+                        const int32_t w = rw[k];
                         ok = ld_level(p.level + w) == lc - 1 && ld_volatile(p.st_inval + w) != p.epoch;
+                        bytes += 8;
                     }
                     found = __any_sync(0xffffffffu, ok);
-                    if (k < clen) bytes += 8;
                 }
                 if (big) {
                     if (lane_id() == 0) {
@@ -611,14 +670,19 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs(BfsParams p) {
             const int clen = (int)min((long long)p.chunk, (long long)r.len - c0);
             const int32_t* rw = p.g.pool + r.start + c0;
             unsigned best = 0xffffffffu;
-            for (int b0 = 0; b0 < clen; b0 += WARP) {
-                int k = b0 + (int)lane_id();
-                if (k < clen) {
-                    int32_t w = rw[k];
-                    if (ld_volatile(p.st_inval + w) != p.epoch) {
-                        int lw = ld_level(p.level + w);
-                        if (lw >= 0) best = min(best, (unsigned)lw);
-                    }
+            for (int b0 = 0; b0 < clen; b0 += PSCAN * WARP) {   // both loads of PSCAN entries in flight
+                int32_t w[PSCAN];
+#pragma unroll
+                for (int u = 0; u < PSCAN; u++) {
+                    const int k = b0 + u * WARP + (int)lane_id();
+                    w[u] = k < clen ? rw[k] : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < PSCAN; u++) {
+                    if (w[u] < 0) continue;
+                    const int32_t si = ld_volatile(p.st_inval + w[u]);
+                    const int lw = ld_level(p.level + w[u]);
+                    if (si != p.epoch && lw >= 0) best = min(best, (unsigned)lw);
                 }
             }
 #pragma unroll

@@ -48,7 +48,8 @@ struct DevCounters {
     int sched_del;            // deletion half-edits
     int decision;             // repair variant the kernels run (read on the device)
     int sort_err;             // 1: a sort look-back wait timed out, 2: a sort position out of range,
-                              // 3: a bulk copy into shared memory (row merge) did not complete
+                              // 3: a bulk copy into shared memory (row merge) did not complete,
+                              // 4: a scan look-back wait timed out
     int sched_flags;          // 1 features computed, 2 model applied
     float feat[24];
     float pred[4];

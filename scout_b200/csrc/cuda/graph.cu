@@ -548,7 +548,7 @@ constexpr int MS_WARPS = 8;
 constexpr int MS_THREADS = MS_WARPS * WARP;
 constexpr int MS_CH = 512;                 // entries per staged chunk
 constexpr int MS_BUF = MS_CH + 8;          // buffer: chunk + 16-byte alignment slack on both ends
-constexpr int MS_ISTAGE = 256;             // insertion keys of one merge step staged per warp
+constexpr int MS_ISTAGE = 448;             // insertion keys of a slice (or one merge step) staged per warp (48 KB static limit)
 constexpr long long MBAR_SPIN_LIMIT = 1ll << 24;
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -580,6 +580,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
     return false;
 }
 
+// First index i in [0, n] with I[i] >= x (I ascending), 32 probes per step (every lane calls
+// it and gets the same answer): a search of a few thousand keys is three dependent loads.
+__device__ __forceinline__ long long warp_lb_key(const KeySpan& I, long long n, int32_t x) {
+    long long lo = 0, hi = n;
+    while (hi - lo > WARP) {
+        const long long step = (hi - lo + WARP - 1) / WARP;
+        const long long pos = lo + (long long)lane_id() * step;
+        const int c = __popc(__ballot_sync(0xffffffffu, pos < hi && I[pos] < x));   // probes below x
+        if (c == 0) { hi = lo; break; }
+        const long long nlo = lo + (long long)(c - 1) * step + 1;
+        hi = min(hi, lo + (long long)c * step);
+        lo = nlo;
+    }
+    const long long pos = lo + lane_id();
+    return lo + __popc(__ballot_sync(0xffffffffu, pos < hi && I[pos] < x));
+}
+
 // First index i in [from, p] with I[i] >= t (I ascending), the warp reading 32 keys per step
 // forward from `from`; every lane calls it and gets the same answer.
 __device__ __forceinline__ long long ins_advance(const KeySpan& I, long long p, long long from, int32_t t) {
@@ -594,14 +611,15 @@ __device__ __forceinline__ long long ins_advance(const KeySpan& I, long long p, 
 
 // Merges old-row entries [b, e) (absolute pool indices) read through `get`, updating the running
 // survivor count; every lane calls it. Survivor x lands at run + (survivors before it in its
-// step) + (insertions < x). The insertions below the step's smallest value are `cur`, which
-// only moves forward along the row (the old entries are ascending): each step advances it to
-// its value range [xmin, xmax) with coalesced reads of the insertion keys, stages the keys of
-// that range in shared memory (s_ins, MS_ISTAGE entries) and searches them there.
+// step) + (insertions < x). With pre >= 0 the slice's whole insertion range I[i0, i0 + pre)
+// is already in s_ins and each survivor searches it there. Otherwise the insertions below the
+// step's smallest value are `cur`, which only moves forward along the row (the old entries are
+// ascending): each step advances it to its value range [xmin, xmax) with coalesced reads of
+// the insertion keys, stages the keys of that range in s_ins when they fit, and searches them.
 template <typename Get>
 __device__ __forceinline__ void merge_span(long long b, long long e, Get get, int32_t* out, long long& run,
                                            const KeySpan& I, long long p, long long& cur, int32_t* s_ins,
-                                           unsigned lt) {
+                                           int pre, long long i0, unsigned lt) {
     constexpr int U = 4;
     for (long long base = b; base < e; base += U * WARP) {
         int32_t x[U];
@@ -609,6 +627,20 @@ __device__ __forceinline__ void merge_span(long long b, long long e, Get get, in
         for (int u = 0; u < U; u++) {
             const long long i = base + u * WARP + lane_id();
             x[u] = i < e ? get(i) : -1;
+        }
+        if (pre >= 0) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool surv = x[u] >= 0;
+                const unsigned m = __ballot_sync(0xffffffffu, surv);
+                if (surv) {
+                    int lo = 0, hi = pre;
+                    while (lo < hi) { const int mid = (lo + hi) >> 1; if (s_ins[mid] < x[u]) lo = mid + 1; else hi = mid; }
+                    out[run + __popc(m & lt) + i0 + lo] = x[u];
+                }
+                run += __popc(m);
+            }
+            continue;
         }
         long long cl = cur, nin = 0;
         if (cur < p) {
@@ -691,15 +723,37 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
         int32_t* out = pool + (in_place_row(p, r.len, long_in_place) ? r.start : tail + off[a]);
         const KeySpan I{keys + b0, B};
         const long long abs0 = r.start + s0, abs1 = r.start + s1;   // pool indices of the slice
-        // insertions below the slice's first value (tombstones keep the value under the sign bit)
-        long long cur = 0;
-        if (s0 > 0 && p > 0) {
-            if (lane_id() == 0) cur = lb_span(I, p, unmark(pool[abs0]));
-            cur = __shfl_sync(0xffffffffu, cur, 0);
+        // The insertions that can land among this slice's entries: I[i0, i1), i0 those below its
+        // first value, i1 those below its last (tombstones keep the value under the sign bit).
+        // When they fit they are staged in shared memory once for the whole slice.
+        long long i0 = 0, i1 = p;
+        if (p > 0) {
+            if (s0 > 0) i0 = warp_lb_key(I, p, unmark(pool[abs0]));
+            if (s1 < r.len) i1 = warp_lb_key(I, p, unmark(pool[abs1 - 1]));
         }
+        const int pre = i1 - i0 <= MS_ISTAGE ? (int)(i1 - i0) : -1;
+        if (pre > 0) {
+            int32_t* si = s_ins[w];
+            for (int j0 = 0; j0 < pre; j0 += 4 * WARP) {
+                int32_t v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int j = j0 + u * WARP + (int)lane_id();
+                    v[u] = j < pre ? I[i0 + j] : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int j = j0 + u * WARP + (int)lane_id();
+                    if (j < pre) si[j] = v[u];
+                }
+            }
+            __syncwarp();
+        }
+        long long cur = i0;
         const bool staged = r.start >= 0 && ((abs1 + 3) & ~3LL) <= pool_cap;
         if (!staged) {
-            merge_span(abs0, abs1, [&](long long i) { return pool[i]; }, out, run, I, p, cur, s_ins[w], lt);
+            merge_span(abs0, abs1, [&](long long i) { return pool[i]; }, out, run, I, p, cur, s_ins[w], pre, i0, lt);
+            __syncwarp();   // s_ins is read before the next slice stages its insertions
             continue;
         }
         const int nch = (int)((s1 - s0 + MS_CH - 1) / MS_CH);
@@ -724,7 +778,7 @@ __global__ void __launch_bounds__(MS_THREADS) k_merge_slices(
             phase[bsel] ^= 1u;
             const long long lo = abs0 + (long long)k * MS_CH, hi = min(abs1, lo + MS_CH);
             const int32_t* sb = s_buf[w][bsel] - (lo & ~3LL);   // indexed by absolute pool index
-            merge_span(lo, hi, [&](long long i) { return sb[i]; }, out, run, I, p, cur, s_ins[w], lt);
+            merge_span(lo, hi, [&](long long i) { return sb[i]; }, out, run, I, p, cur, s_ins[w], pre, i0, lt);
             __syncwarp();   // every lane is done with this buffer before it is refilled
             if (k + 2 < nch && lane_id() == 0) {
                 fence_proxy_async_smem();   // the warp's reads of the buffer precede the copy's writes
@@ -997,6 +1051,7 @@ int counters_fetch(scout_ctx* c) {
                                       "(an edge joins two labels); upload a consistent labelling");
     if (c->h_ctr->sort_err == 1) return c->fail(SCOUT_E_TIMEOUT, "a sort look-back wait timed out");
     if (c->h_ctr->sort_err == 3) return c->fail(SCOUT_E_TIMEOUT, "a bulk copy of a row slice into shared memory did not complete");
+    if (c->h_ctr->sort_err == 4) return c->fail(SCOUT_E_TIMEOUT, "a scan look-back wait timed out");
     if (c->h_ctr->sort_err) return c->fail(SCOUT_E_STATE, "the sort computed a position out of range");
     if (c->h_bar->err != 0 || c->h_ctr->overflow)
         return c->fail(SCOUT_E_CAPACITY, "a device work list overflowed its capacity");

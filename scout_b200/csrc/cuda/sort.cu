@@ -263,103 +263,96 @@ __device__ __forceinline__ long long block_excl_scan(long long x, long long* tot
     return r;
 }
 
-template <typename T>
-__global__ void k_scan_tiles(const T* __restrict__ a, int64_t n, int64_t* __restrict__ sums) {
-    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
-    long long s = 0;
-    for (int k = 0; k < SCAN_ITEMS; k++)
-        if (base + k < n) s += (long long)a[base + k];
-    __shared__ long long tot;
-    block_excl_scan(s, &tot);
-    __syncthreads();
-    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
-}
-
-__global__ void k_scan_sums(int64_t* __restrict__ sums, int64_t nb, int64_t* __restrict__ d_total) {
-    __shared__ long long part[1024];
-    int t = threadIdx.x, T = blockDim.x;
-    int64_t per = (nb + T - 1) / T;
-    int64_t lo = (int64_t)t * per, hi = lo + per < nb ? lo + per : nb;
-    long long s = 0;
-    for (int64_t i = lo; i < hi; i++) s += sums[i];
-    part[t] = s;
-    __syncthreads();
-    for (int o = 1; o < T; o <<= 1) {
-        long long y = t >= o ? part[t - o] : 0;
-        __syncthreads();
-        part[t] += y;
-        __syncthreads();
-    }
-    long long run = part[t] - s;
-    for (int64_t i = lo; i < hi; i++) {
-        long long x = sums[i];
-        sums[i] = run;
-        run += x;
-    }
-    if (t == T - 1 && d_total) *d_total = part[T - 1];
-}
+// Single-pass exclusive scan (decoupled look-back, after Merrill and Garland, "Single-pass
+// parallel prefix scan with decoupled look-back", 2016). Tiles of SCAN_TILE entries take
+// tickets in order from a counter; a tile publishes its aggregate, its first warp walks back
+// over the earlier tiles 32 at a time (adding aggregates up to the nearest published inclusive
+// prefix) and publishes its own prefix, then the block writes its exclusive prefixes. One launch for any
+// length. State in st (64-bit words): [0] the ticket counter, then per tile a status word
+// (LB_TAG | stamp << 2 | flag; flag 1 aggregate, 2 inclusive prefix), the aggregate and the
+// prefix. The stamp is unique per call, so no state is cleared between calls. A wait past
+// LB_WAIT_LIMIT_NS flags err = 4 (the host fails the batch) and the tile goes on.
+constexpr unsigned long long LB_TAG = 0xA5ull << 56;
+constexpr uint64_t LB_WAIT_LIMIT_NS = 1000000000ull;   // 1 s
 
 template <typename T>
-__global__ void k_scan_apply(T* __restrict__ a, int64_t n, const int64_t* __restrict__ sums) {
-    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_lb(T* __restrict__ a, int64_t n, int64_t* __restrict__ d_total,
+                                                          unsigned long long* __restrict__ st, unsigned stamp,
+                                                          int* __restrict__ err) {
+    __shared__ int s_tile;
+    __shared__ long long s_tot, s_prefix;
+    if (threadIdx.x == 0) s_tile = (int)atomicAdd((unsigned*)st, 1u);
+    __syncthreads();
+    const int tile = s_tile;
+    const int64_t base = (int64_t)tile * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
     long long v[SCAN_ITEMS];
-    long long s = 0;
+    long long sum = 0;
+#pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
         v[k] = base + k < n ? (long long)a[base + k] : 0;
-        s += v[k];
+        sum += v[k];
     }
-    long long ex = block_excl_scan(s, nullptr) + sums[blockIdx.x];
+    const long long ex = block_excl_scan(sum, &s_tot);
+    if (threadIdx.x < WARP) {   // warp 0: publish, look back 32 tiles per step, publish the prefix
+        const long long tot = s_tot;
+        const unsigned long long want = LB_TAG | ((unsigned long long)stamp << 2);
+        unsigned long long* me = st + 1 + 3 * (int64_t)tile;
+        const int lane = (int)threadIdx.x;
+        long long prefix = 0;
+        if (tile > 0) {
+            if (lane == 0) {
+                me[1] = (unsigned long long)tot;
+                __threadfence();
+                *(volatile unsigned long long*)me = want | 1ull;
+            }
+            const uint64_t t0 = globaltimer_ns();
+            for (long long end = tile - 1;; end -= WARP) {
+                const long long j = end - lane;   // lane 0 looks at the nearest tile
+                unsigned long long w = want | 2ull;   // tiles before the first: a prefix of 0
+                bool ok = true;
+                if (j >= 0) {
+                    const unsigned long long* pj = st + 1 + 3 * j;
+                    w = ld_volatile(pj);
+                    for (unsigned it = 1; (w & ~3ull) != want || (w & 3ull) == 0; it++) {
+                        if ((it & 63) == 0 && globaltimer_ns() - t0 > LB_WAIT_LIMIT_NS) { ok = false; break; }
+                        w = ld_volatile(pj);
+                    }
+                }
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicCAS(err, 0, 4);
+                    break;
+                }
+                __threadfence();
+                const bool pre = (w & 3ull) == 2;
+                long long v = 0;
+                if (j >= 0) v = (long long)ld_volatile(st + 1 + 3 * j + (pre ? 2 : 1));
+                const unsigned pm = __ballot_sync(0xffffffffu, pre);
+                const int f = pm ? __ffs(pm) - 1 : WARP;   // nearest tile with an inclusive prefix
+                if (lane > f) v = 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                prefix += v;
+                if (pm) break;
+            }
+        }
+        if (lane == 0) {
+            me[2] = (unsigned long long)(prefix + tot);
+            __threadfence();
+            *(volatile unsigned long long*)me = want | 2ull;
+            s_prefix = prefix;
+            if (d_total && (int64_t)(tile + 1) * SCAN_TILE >= n) *d_total = prefix + tot;
+        }
+    }
+    __syncthreads();
+    long long run = s_prefix + ex;
+#pragma unroll
     for (int k = 0; k < SCAN_ITEMS; k++) {
-        if (base + k < n) a[base + k] = (T)ex;
-        ex += v[k];
+        if (base + k < n) a[base + k] = (T)run;
+        run += v[k];
     }
 }
 
-// Arrays of up to SCAN_ONE_MAX entries are scanned by one 1024-thread block in one launch, in
-// steps of SCAN_ONE_STEP entries: each thread loads SCAN_ONE_IPT consecutive entries (a warp
-// reads one contiguous 2 KB span), the block scans the thread sums, and a running carry links
-// the steps. Longer arrays take the three-launch tile scan.
-constexpr int64_t SCAN_ONE_MAX = 1 << 16;
-constexpr int SCAN_ONE_THREADS = 1024;
-constexpr int SCAN_ONE_IPT = 8;
-constexpr int SCAN_ONE_STEP = SCAN_ONE_THREADS * SCAN_ONE_IPT;
-
-template <typename T>
-__global__ void __launch_bounds__(SCAN_ONE_THREADS) k_scan_one(T* __restrict__ a, int64_t n, int64_t* __restrict__ d_total) {
-    __shared__ long long ws[SCAN_ONE_THREADS / WARP];
-    __shared__ long long s_step;
-    const int t = threadIdx.x, w = t / WARP, lane = t & (WARP - 1);
-    long long carry = 0;
-    for (int64_t base = 0; base < n; base += SCAN_ONE_STEP) {
-        const int64_t i0 = base + (int64_t)t * SCAN_ONE_IPT;
-        long long x[SCAN_ONE_IPT];
-        long long s = 0;
-#pragma unroll
-        for (int k = 0; k < SCAN_ONE_IPT; k++) {
-            x[k] = i0 + k < n ? (long long)a[i0 + k] : 0;
-            s += x[k];
-        }
-        const long long inc = warp_incl_scan(s);
-        if (lane == WARP - 1) ws[w] = inc;
-        __syncthreads();
-        if (w == 0) {
-            const long long v = ws[lane];
-            const long long vi = warp_incl_scan(v);
-            ws[lane] = vi - v;
-            if (lane == WARP - 1) s_step = vi;
-        }
-        __syncthreads();
-        long long run = carry + ws[w] + inc - s;
-#pragma unroll
-        for (int k = 0; k < SCAN_ONE_IPT; k++) {
-            if (i0 + k < n) a[i0 + k] = (T)run;
-            run += x[k];
-        }
-        carry += s_step;
-        __syncthreads();   // ws and s_step are read before the next step writes them
-    }
-    if (t == 0 && d_total) *d_total = carry;
-}
+static unsigned next_stamp();
 
 template <typename T>
 static int scan_any(scout_ctx* c, T* data, int64_t n, int64_t* d_total) {
@@ -367,19 +360,13 @@ static int scan_any(scout_ctx* c, T* data, int64_t n, int64_t* d_total) {
         if (d_total) SCOUT_CU(c, cudaMemsetAsync(d_total, 0, sizeof(int64_t), c->s_main));
         return SCOUT_OK;
     }
-    if (n <= SCAN_ONE_MAX) {
-        k_scan_one<T><<<1, SCAN_ONE_THREADS, 0, c->s_main>>>(data, n, d_total);
-        SCOUT_LAUNCH(c, "k_scan_one");
-        c->nlaunch += 1;
-        return SCOUT_OK;
-    }
-    int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
-    SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, nb + 1, "scan partials"));
-    k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
-    k_scan_sums<<<1, 1024, 0, c->s_main>>>(c->d_scan_tmp, nb, d_total);
-    k_scan_apply<T><<<(unsigned)nb, SCAN_THREADS, 0, c->s_main>>>(data, n, c->d_scan_tmp);
-    SCOUT_LAUNCH(c, "scan");
-    c->nlaunch += 3;
+    const int64_t nt = (n + SCAN_TILE - 1) / SCAN_TILE;
+    SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, std::max<int64_t>(64, 1 + 3 * nt), "scan look-back"));
+    SCOUT_CU(c, cudaMemsetAsync(c->d_scan_tmp, 0, sizeof(int64_t), c->s_main));   // tile tickets
+    k_scan_lb<T><<<(unsigned)nt, SCAN_THREADS, 0, c->s_main>>>(data, n, d_total, (unsigned long long*)c->d_scan_tmp,
+                                                                next_stamp(), &c->d_ctr->sort_err);
+    SCOUT_LAUNCH(c, "k_scan_lb");
+    c->nlaunch += 1;
     return SCOUT_OK;
 }
 
@@ -402,7 +389,8 @@ int sort_reserve(scout_ctx* c, int64_t nkeys) {
     if (c->d_sort_hist != before)   // fresh memory: no stale look-back entry may match a stamp
         SCOUT_CU(c, cudaMemsetAsync(c->d_sort_hist, 0, (size_t)c->cap_hist * 4, c->s_main));
     const int64_t scan_n = nkeys + 1;
-    SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, (scan_n + SCAN_TILE - 1) / SCAN_TILE + 1, "scan partials"));
+    SCOUT_RC(dev_grow(c, &c->d_scan_tmp, &c->cap_scan, std::max<int64_t>(64, 1 + 3 * ((scan_n + SCAN_TILE - 1) / SCAN_TILE)),
+                      "scan look-back"));
     return SCOUT_OK;
 }
 
