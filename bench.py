@@ -640,8 +640,9 @@ def multi_workload(nbatches: int, seed: int = 7):
 
 def multi_stream(a, device, model, tuned):
     """Plain (one context per stream, batches one at a time in arrival order), batched (one
-    union store per problem, rounds) and learned+batched (the same with the scheduler model)
-    on the same 64-stream workload. Times: device CUDA events of the library per batch or round
+    union store per problem, rounds), learned+batched (the same with the scheduler model) and
+    fused (the four union stores at once, one repair launch per round across problems) on the
+    same 64-stream workload. Times: device CUDA events of the library per batch or round
     (edits already copied), and host wall time of the synchronous calls (copies in, commit out)."""
     import scout_b200 as sb
     graphs, streams, arrivals = multi_workload(a.multi_batches)
@@ -714,11 +715,50 @@ def multi_stream(a, device, model, tuned):
             res[arm]["wall_ms"] += 1e3 * (time.perf_counter() - t0)
             res[arm]["rounds"] += len(rounds)
             me.close()
+    # fused: the four union stores at once; a round's four merges, then ONE persistent kernel
+    # running the four repairs (scout_multi_run_all), the rounds of each problem as above
+    res["fused"] = {"dev_ms": 0.0, "wall_ms": 0.0, "lat": [], "rounds": 0}
+    engines, mirs, rounds_p, pinned_all = {}, {}, {}, {}
+    cap = int(tuned.get("round_cap", 1 << 21))
+    sched = launch_knobs(tuned.get("bfs", {}))
+    for p in MULTI_PROBLEMS:
+        sids = [i for i, st in enumerate(streams) if st["problem"] == p]
+        arr_p = [(i, j) for i, j in arrivals if streams[i]["problem"] == p]
+        me = sb.MultiEngine(p, device, budget_bytes=36 << 30)   # four stores side by side
+        local = {}
+        for i in sids:
+            off, adj = arrays[streams[i]["graph"]]
+            local[i] = me.add_stream(off, adj, inits[(p, streams[i]["graph"])], 0)
+        me.seal()
+        pinned_all[p] = {(i, j): sb.pinned_copy(streams[i]["batches"][j]) for i, j in arr_p}
+        me.reserve_batches(max(cap, max(len(b) for b in pinned_all[p].values())))
+        engines[p] = me
+        mirs[p] = [inits[(p, streams[i]["graph"])].copy() for i in sids]
+        rounds_p[p] = sb.form_rounds([(local[i], pinned_all[p][(i, j)]) for i, j in arr_p], cap)
+    nr = max(len(r) for r in rounds_p.values())
+    t0 = time.perf_counter()
+    for r in range(nr):
+        members = [p for p in MULTI_PROBLEMS if r < len(rounds_p[p])]
+        t1 = time.perf_counter()
+        for p in members:
+            engines[p].stage(rounds_p[p][r])
+        sts = sb.run_fused_round([engines[p] for p in members], sched=sched)
+        for p in members:
+            engines[p].commit(mirs[p])
+        dt = 1e3 * (time.perf_counter() - t1)
+        res["fused"]["lat"] += [dt] * sum(len(rounds_p[p][r]) for p in members)
+        res["fused"]["dev_ms"] += sum(x["ms_compact"] + x["ms_update"] for x in sts) + sts[0]["ms_repair"]
+    res["fused"]["wall_ms"] = 1e3 * (time.perf_counter() - t0)
+    res["fused"]["rounds"] = nr
+    for me in engines.values():
+        me.close()
+    arms["fused"] = None
     for arm, r in res.items():
         out[arm] = {"edge_updates_per_s": total_edits / (r["dev_ms"] / 1e3),
                     "e2e_edge_updates_per_s": total_edits / (r["wall_ms"] / 1e3),
                     "p50_batch_ms": float(np.percentile(r["lat"], 50)),
-                    "p99_batch_ms": float(np.percentile(r["lat"], 99)), "launch_rounds": r["rounds"]}
+                    "p99_batch_ms": float(np.percentile(r["lat"], 99)),
+                    ("repair_launches" if arm == "fused" else "launch_rounds"): r["rounds"]}
     base = out["plain"]["e2e_edge_updates_per_s"]
     for arm in arms:
         out[arm]["e2e_vs_plain"] = out[arm]["e2e_edge_updates_per_s"] / base

@@ -303,6 +303,16 @@ int scout_multi_probe(scout_multi* m, int32_t k, const int32_t* stream_ids, cons
                       double* variant_ms, float* features, scout_batch_stats* stats);
 /* Changed entries of the last round into per-stream host mirrors (mirrors[k]: n_k entries, or
  * NULL to skip stream k); *changed receives the number of entries that changed. */
+/* A round of several engines of distinct problems (at most one per problem, one device)
+ * repaired by ONE persistent kernel: each engine's round is assembled by scout_multi_stage
+ * (the arguments of scout_multi_round), then scout_multi_run_all merges every staged round
+ * into its engine's store (on its own stream) and runs one cooperative launch in which the
+ * engines' repairs follow one another, each over its own store with its own counters and
+ * bounded grid barrier. stats: ne entries (ms_repair is the shared launch); repairs use their
+ * plain variants. Commit each engine with scout_multi_commit as after scout_multi_round. */
+int scout_multi_stage(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops);
+int scout_multi_run_all(int32_t ne, scout_multi* const* ms, const scout_sched* sched, scout_batch_stats* stats);
 int scout_multi_commit(scout_multi* m, int32_t* const* mirrors, int64_t* changed);
 /* One stream's current solution (n = the stream's vertex count). */
 int scout_multi_download(scout_multi* m, int32_t stream, int32_t* out, int64_t n);

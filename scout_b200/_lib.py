@@ -113,6 +113,8 @@ SIGNATURES = [
                                     C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
     ("scout_multi_probe", C.c_int, [_vp, C.c_int32, _i32p, C.POINTER(_edgep), _i64p, C.POINTER(_u8p),
                                     C.POINTER(ScoutSched), _f64p, _f32p, C.POINTER(ScoutBatchStats)]),
+    ("scout_multi_stage", C.c_int, [_vp, C.c_int32, _i32p, C.POINTER(_edgep), _i64p, C.POINTER(_u8p)]),
+    ("scout_multi_run_all", C.c_int, [C.c_int32, C.POINTER(_vp), C.POINTER(ScoutSched), C.POINTER(ScoutBatchStats)]),
     ("scout_multi_commit", C.c_int, [_vp, C.POINTER(_i32p), _i64p]),
     ("scout_multi_download", C.c_int, [_vp, C.c_int32, _i32p, C.c_int64]),
     ("scout_multi_streams", C.c_int, [_vp, _i32p, _i64p]),

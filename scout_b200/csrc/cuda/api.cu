@@ -86,6 +86,7 @@ static void release(scout_ctx* c) {
     if (c->ev_gather0) cudaEventDestroy(c->ev_gather0);
     if (c->ev_gather1) cudaEventDestroy(c->ev_gather1);
     if (c->ev_pf) cudaEventDestroy(c->ev_pf);
+    if (c->ev_union) cudaEventDestroy(c->ev_union);
     void* gdev[] = {c->gather_stamp, c->d_gctr, c->d_pf_edits[0], c->d_pf_edits[1], c->d_gather_list, c->d_gather_dst};
     for (void* p : gdev) if (p) cudaFree(p);
     if (c->h_gctr) cudaFreeHost(c->h_gctr);
@@ -186,6 +187,7 @@ int scout_ctx_create(int device, uint64_t budget, scout_ctx** out) {
     for (int i = 0; i < 8 && ok; i++) ok = cudaEventCreate(&c->ev_t[i]) == cudaSuccess;
     ok = ok && cudaEventCreate(&c->ev_gather0) == cudaSuccess && cudaEventCreate(&c->ev_gather1) == cudaSuccess;
     ok = ok && cudaEventCreateWithFlags(&c->ev_pf, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&c->ev_union, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaMallocHost((void**)&c->h_ctr, sizeof(DevCounters)) == cudaSuccess &&
          cudaMallocHost((void**)&c->h_bar, sizeof(GridBar)) == cudaSuccess;
     if (!ok) { cudaError_t le = cudaGetLastError(); release(c); return cuda_fail(nullptr, le, "context streams"); }
@@ -387,6 +389,56 @@ __global__ void k_count_diff(const int32_t* __restrict__ a, const int32_t* __res
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
     if ((threadIdx.x & 31) == 0 && d) atomicAdd(cnt, d);
+}
+
+// One round of several union stores of distinct problems (ne <= 4, one device): every batch is
+// merged on its store's stream, then ONE cooperative launch runs all the repairs (union.cu),
+// then each store's counters are read into its stats (ms_repair: the shared launch). The
+// repairs run their plain variants; the learned scheduler decides per launch and is not used.
+int union_run(scout_ctx* const* cs, const int* problems, const scout_edge* const* edits, const uint8_t* const* ops,
+              const int64_t* counts, int ne, const scout_sched* sched, scout_batch_stats* stats) {
+    if (ne < 1 || ne > 4 || !cs || !problems || !edits || !counts || !stats) return host_fail(SCOUT_E_INVALID, "bad round arguments");
+    for (int i = 0; i < ne; i++) {
+        if (!cs[i]) return host_fail(SCOUT_E_INVALID, "null engine");
+        if (cs[i]->device != cs[0]->device) return cs[i]->fail(SCOUT_E_INVALID, "the engines of a fused round share one device");
+        for (int j = 0; j < i; j++)
+            if (problems[j] == problems[i] || cs[j] == cs[i])
+                return cs[i]->fail(SCOUT_E_INVALID, "a fused round takes one engine per problem");
+        if (counts[i] < 0 || (counts[i] > 0 && !edits[i])) return cs[i]->fail(SCOUT_E_INVALID, "bad batch");
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    scout_sched sds[4];
+    int variants[4];
+    int64_t launch0[4];
+    for (int i = 0; i < ne; i++) {
+        std::memset(&sds[i], 0, sizeof(scout_sched));
+        if (sched) sds[i] = *sched;
+        sds[i].policy = SCOUT_SCHED_PLAIN;
+        SCOUT_RC(apply_tuning(cs[i], sds[i]));
+        launch0[i] = cs[i]->nlaunch;
+        SCOUT_RC(batch_prologue(cs[i], problems[i], edits[i], ops ? ops[i] : nullptr, counts[i], &stats[i]));
+        variants[i] = plain_variant(problems[i], sds[i]);
+    }
+    SCOUT_RC(union_launch(cs, problems, sds, variants, ne));
+    for (int i = 0; i < ne; i++) {
+        scout_ctx* c = cs[i];
+        SCOUT_CU(c, cudaEventRecord(c->ev_t[2], c->s_main));
+        SCOUT_RC(counters_fetch(c));
+        const DevCounters& h = *c->h_ctr;
+        advance_tails(c, h);
+        c->nnz += h.nnz_delta;
+        c->qtag += (uint32_t)h.rounds + 8;
+        fill_stats(c, &stats[i], launch0[i]);
+        stats[i].variant = variants[i];
+    }
+    const double ms = ev_ms(cs[0]->ev_t[4], cs[0]->ev_t[5]);
+    const double total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (int i = 0; i < ne; i++) {
+        stats[i].ms_repair = ms;
+        stats[i].ms_total = total;
+        cs[i]->prev_repair_ms[problems[i]] = ms;
+    }
+    return SCOUT_OK;
 }
 
 }  // namespace scout

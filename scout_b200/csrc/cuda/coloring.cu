@@ -13,191 +13,12 @@
 // barrier: propose (warp per row up to 4096 entries, whole block per longer row, colours
 // gathered into a shared-memory bitmap of 1024-colour windows), detect, apply.
 #include "ctx.cuh"
+#include "coloring_dev.cuh"
 
 namespace scout {
 
-constexpr int COL_THREADS = 256;
-constexpr int COL_WIN = 1024;            // colours per bitmap window
-constexpr int COL_WORDS = COL_WIN / 32;
-constexpr int COL_BIG = 4096;            // rows longer than this are processed by a whole block
-constexpr int32_t UNMARKED = -2;
+__global__ void __launch_bounds__(COL_THREADS) k_coloring(ColParams p) { coloring_body(p); }
 
-struct ColParams {
-    DGraph g;
-    int32_t* color;
-    int32_t* marker;     // proposal of round vertices, UNMARKED elsewhere (persistent)
-    const unsigned long long* hkeys;
-    int B;
-    int32_t* list[2];    // round vertex lists (n each)
-    int32_t* prop;       // proposal per list index
-    int32_t* touched;
-    int32_t* st_round;   // dedupe of the initial marking (epoch)
-    int32_t* st_touch;
-    int32_t epoch;
-    DevCounters* ctr;
-    GridBar* bar;
-};
-
-struct WarpSync {
-    __device__ void operator()() const { __syncwarp(); }
-};
-struct BlockSync {
-    __device__ void operator()() const { __syncthreads(); }
-};
-
-// Smallest colour absent from the neighbours of x, scanned by `lanes` threads of a group whose
-// shared bitmap is `bm` (COL_WORDS words). `sync` synchronises the group.
-template <typename Sync>
-__device__ int smallest_free(const ColParams& p, int32_t x, int tid, int lanes, unsigned* bm, Sync sync,
-                             int* s_res, long long& bytes) {
-    Row r = p.g.row[x];
-    const int32_t* rw = p.g.pool + r.start;
-    for (int base = 0;; base += COL_WIN) {
-        for (int k = tid; k < COL_WORDS; k += lanes) bm[k] = 0;
-        sync();
-        for (long long i = tid; i < r.len; i += lanes) {
-            int c = ld_volatile(p.color + rw[i]);
-            if (c >= base && c < base + COL_WIN) atomicOr(&bm[(c - base) >> 5], 1u << ((c - base) & 31));
-        }
-        bytes += 8LL * ((r.len + lanes - 1 - tid) / lanes);
-        sync();
-        if (tid == 0) *s_res = -1;
-        sync();
-        for (int k = tid; k < COL_WORDS; k += lanes) {
-            unsigned free_bits = ~bm[k];
-            if (free_bits) atomicMin((unsigned*)s_res, (unsigned)(k * 32 + __ffs(free_bits) - 1));
-        }
-        sync();
-        int res = *s_res;
-        sync();
-        if (res >= 0) return base + res;
-    }
-}
-
-__global__ void __launch_bounds__(COL_THREADS) k_coloring(ColParams p) {
-    __shared__ unsigned s_bm[COL_THREADS / WARP][COL_WORDS];
-    __shared__ int s_res[COL_THREADS / WARP];
-    __shared__ unsigned s_bbm[COL_WORDS];
-    __shared__ int s_bres;
-    __shared__ int s_flag;
-    const int W = gwarp_count(), wid = gwarp_id(), wl = threadIdx.x / WARP;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t T = (int64_t)gridDim.x * blockDim.x;
-    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
-    long long bytes = 0;
-    int rounds = 0;
-
-    // ---- marking: higher endpoint of every same-colour inserted edge (pre-batch colours) ----
-    const int nh = ld_volatile(&p.ctr->n_half);
-    for (int64_t b = tid - (tid & (WARP - 1)); b < nh; b += T) {
-        int64_t k = b + lane_id();
-        bool mark = false, conflict = false;
-        int32_t loser = 0;
-        if (k < nh) {
-            unsigned long long key = p.hkeys[k];
-            int op = (int)((key >> p.B) & 1ull);
-            int32_t x = (int32_t)(key >> (p.B + 1));
-            int32_t y = (int32_t)(key & ((1ull << p.B) - 1));
-            if (op == 0 && x < y && ld_volatile(p.color + x) == ld_volatile(p.color + y)) {
-                conflict = true;
-                loser = y;
-                mark = atomicExch(&p.st_round[y], p.epoch) != p.epoch;
-            }
-        }
-        unsigned mc = __ballot_sync(0xffffffffu, conflict);
-        if (lane_id() == 0 && mc) atomicAdd(&p.ctr->conflicts, __popc(mc));
-        int at = warp_append(mark, &p.ctr->list_count[0]);
-        if (mark) p.list[0][at] = loser;
-    }
-    if (!grid_sync(p.bar, 10)) return;
-
-    int cur = 0;
-    while (true) {
-        const int cnt = ld_volatile(&p.ctr->list_count[cur]);
-        if (cnt == 0) break;
-        const int nxt = cur ^ 1;
-        // ---- propose ----
-        if (leader) p.ctr->list_count[nxt] = 0;   // nobody reads it until the detect phase
-        for (int i = wid; i < cnt; i += W) {   // rows up to COL_BIG: one warp
-            int32_t x = p.list[cur][i];
-            if (p.g.row[x].len > COL_BIG) continue;
-            int c = smallest_free(p, x, (int)lane_id(), WARP, s_bm[wl], WarpSync(), &s_res[wl], bytes);
-            if (lane_id() == 0) { p.prop[i] = c; p.marker[x] = c; }
-        }
-        for (int i = blockIdx.x; i < cnt; i += gridDim.x) {   // longer rows: one block
-            int32_t x = p.list[cur][i];
-            if (p.g.row[x].len <= COL_BIG) continue;
-            int c = smallest_free(p, x, threadIdx.x, COL_THREADS, s_bbm, BlockSync(), &s_bres, bytes);
-            if (threadIdx.x == 0) { p.prop[i] = c; p.marker[x] = c; }
-            __syncthreads();
-        }
-        if (!grid_sync(p.bar, 11)) return;
-        // ---- detect: a lower-id round neighbour proposed the same colour ----
-        for (int i = wid; i < cnt; i += W) {
-            int32_t x = p.list[cur][i];
-            Row r = p.g.row[x];
-            if (r.len > COL_BIG) continue;
-            const int32_t* rw = p.g.pool + r.start;
-            int c = p.prop[i];
-            bool lose = false;
-            for (int b0 = 0; b0 < r.len && !lose; b0 += WARP) {
-                int k = b0 + (int)lane_id();
-                bool l2 = false;
-                if (k < r.len) {
-                    int32_t w = rw[k];
-                    l2 = w < x && ld_volatile(p.marker + w) == c;
-                }
-                lose = __any_sync(0xffffffffu, l2);
-                if (k < r.len) bytes += 8;
-            }
-            int at = warp_append(lane_id() == 0 && lose, &p.ctr->list_count[nxt]);
-            if (lane_id() == 0 && lose) p.list[nxt][at] = x;
-        }
-        for (int i = blockIdx.x; i < cnt; i += gridDim.x) {
-            int32_t x = p.list[cur][i];
-            Row r = p.g.row[x];
-            if (r.len <= COL_BIG) continue;
-            const int32_t* rw = p.g.pool + r.start;
-            int c = p.prop[i];
-            if (threadIdx.x == 0) s_flag = 0;
-            __syncthreads();
-            for (long long k = threadIdx.x; k < r.len; k += COL_THREADS) {
-                int32_t w = rw[k];
-                if (w < x && ld_volatile(p.marker + w) == c) s_flag = 1;
-            }
-            bytes += 8LL * ((r.len + COL_THREADS - 1 - threadIdx.x) / COL_THREADS);
-            __syncthreads();
-            if (threadIdx.x == 0 && s_flag) p.list[nxt][atomicAdd(&p.ctr->list_count[nxt], 1)] = x;
-            __syncthreads();
-        }
-        if (!grid_sync(p.bar, 12)) return;
-        // ---- apply all proposals, clear markers, record touched vertices ----
-        for (int64_t b = tid - (tid & (WARP - 1)); b < cnt; b += T) {
-            int64_t i = b + lane_id();
-            bool nt = false;
-            int32_t x = 0;
-            if (i < cnt) {
-                x = p.list[cur][i];
-                p.color[x] = p.prop[i];
-                p.marker[x] = UNMARKED;
-                nt = atomicExch(&p.st_touch[x], p.epoch) != p.epoch;
-                bytes += 16;
-            }
-            int at = warp_append(nt, &p.ctr->changed);
-            if (nt) p.touched[at] = x;
-        }
-        rounds++;
-        if (!grid_sync(p.bar, 13)) return;
-        cur = nxt;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-    if (lane_id() == 0) atomicAdd((unsigned long long*)&p.ctr->hbm_bytes, (unsigned long long)bytes);
-    if (leader) {
-        p.ctr->rounds = rounds;
-        p.ctr->affected = p.ctr->changed;
-    }
-}
 
 __global__ void k_fill_marker(int32_t* __restrict__ m, int64_t n) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
@@ -217,11 +38,11 @@ int coloring_ensure(scout_ctx* c) {
     return SCOUT_OK;
 }
 
-int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
-    (void)st;
+// The kernel's parameters for the context's current batch (buffers ensured first).
+int coloring_params(scout_ctx* c, ColParams* out) {
     SCOUT_RC(lists_ensure(c));
     SCOUT_RC(coloring_ensure(c));
-    ColParams p;
+    ColParams& p = *out;
     p.g = dgraph(c);
     p.color = c->color;
     p.marker = (int32_t*)c->d_misc;
@@ -236,6 +57,13 @@ int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
     p.epoch = (int32_t)c->epoch;
     p.ctr = c->d_ctr;
     p.bar = c->d_bar;
+    return SCOUT_OK;
+}
+
+int coloring_repair(scout_ctx* c, scout_batch_stats* st) {
+    (void)st;
+    ColParams p;
+    SCOUT_RC(coloring_params(c, &p));
     void* args[] = {&p};
     return coop_launch(c, (const void*)k_coloring, COL_THREADS, args, 0);
 }

@@ -101,6 +101,7 @@ struct scout_ctx {
     int64_t pf_ready_m = 0;
     bool pf_use = false;            // this call's edits are the hinted batch (scout_sched.prefetched)
     cudaEvent_t ev_pf = nullptr;    // the hinted edits' copy is done (copy stream)
+    cudaEvent_t ev_union = nullptr; // fused repair rounds: this store's merge / the repair is done
     int32_t* gather_stamp = nullptr;   // n: last gather that took the vertex's row
     uint32_t gather_tag = 0;
     void* d_gctr = nullptr;
@@ -296,6 +297,11 @@ int coop_launch(scout_ctx* c, const void* fn, int threads, void** args, size_t s
 // free HBM from `base` on a copy stream, after the current merge is queued; gather_finish waits
 // for the gather (main stream and host) and moves the tail.
 int prefetch_launch(scout_ctx* c, long long base);
+// union.cu: one cooperative launch of the repairs of ne union stores of distinct problems whose
+// batches are merged (queued); api.cu: the whole round (merges, launch, counters, stats)
+int union_launch(scout_ctx* const* cs, const int* problems, const scout_sched* sds, const int* variants, int ne);
+int union_run(scout_ctx* const* cs, const int* problems, const scout_edge* const* edits, const uint8_t* const* ops,
+              const int64_t* counts, int ne, const scout_sched* sched, scout_batch_stats* stats);
 // graph.cu: host copy into page-locked staging, over the host threads for large copies
 void stage_copy(void* dst, const void* src, size_t bytes);
 int gather_finish(scout_ctx* c, double* ms, int64_t* rows, int64_t* bytes);

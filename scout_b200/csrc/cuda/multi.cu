@@ -40,6 +40,9 @@ struct scout_multi {
     std::vector<int64_t> bases;   // stream bases, ascending
     int64_t total_n = 0;
     bool sealed = false;
+    bool staged = false;          // a round is assembled in pin for scout_multi_run_all
+    int64_t staged_total = 0;
+    bool staged_ops = false;
     scout_edge* pin = nullptr;    // page-locked union batch
     uint8_t* pin_ops = nullptr;
     int64_t pin_cap = 0;
@@ -230,6 +233,40 @@ int scout_multi_round(scout_multi* m, int32_t k, const int32_t* stream_ids, cons
     bool any_ops = false;
     SCOUT_RC(assemble(m, k, stream_ids, edits, counts, ops, &total, &any_ops));
     return scout_repair(m->ctx, m->problem, m->pin, any_ops ? m->pin_ops : nullptr, total, sched, stats);
+}
+
+int scout_multi_stage(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,
+                      const int64_t* counts, const uint8_t* const* ops) {
+    int64_t total = 0;
+    bool any_ops = false;
+    if (m) m->staged = false;
+    SCOUT_RC(assemble(m, k, stream_ids, edits, counts, ops, &total, &any_ops));
+    m->staged = true;
+    m->staged_total = total;
+    m->staged_ops = any_ops;
+    return SCOUT_OK;
+}
+
+int scout_multi_run_all(int32_t ne, scout_multi* const* ms, const scout_sched* sched, scout_batch_stats* stats) {
+    if (ne < 1 || ne > 4 || !ms || !stats) return host_fail(SCOUT_E_INVALID, "bad round arguments");
+    scout_ctx* cs[4];
+    int problems[4];
+    const scout_edge* edits[4];
+    const uint8_t* ops[4];
+    int64_t counts[4];
+    for (int i = 0; i < ne; i++) {
+        scout_multi* m = ms[i];
+        if (!m || !m->staged) return mfail(m, SCOUT_E_STATE, "every engine of a fused round needs a staged round");
+        cs[i] = m->ctx;
+        problems[i] = m->problem;
+        edits[i] = m->pin;
+        ops[i] = m->staged_ops ? m->pin_ops : nullptr;
+        counts[i] = m->staged_total;
+        std::memset(&stats[i], 0, sizeof(scout_batch_stats));
+    }
+    const int rc = union_run(cs, problems, edits, ops, counts, ne, sched, stats);
+    for (int i = 0; i < ne; i++) ms[i]->staged = false;
+    return rc;
 }
 
 int scout_multi_probe(scout_multi* m, int32_t k, const int32_t* stream_ids, const scout_edge* const* edits,

@@ -394,6 +394,15 @@ class MultiEngine:
         self._c(LIB.scout_multi_round(self._h, k, _p32(ids), ptrs, _p64(counts), None, C.byref(sd), C.byref(st)))
         return st.as_dict()
 
+    def stage(self, batches) -> None:
+        """Assemble a round ([(stream_id, edges), ...]) for run_fused_round."""
+        k = len(batches)
+        ids = np.array([s for s, _ in batches], dtype=np.int32)
+        arrs = [as_edges(b) for _, b in batches]
+        ptrs = (C.POINTER(ScoutEdge) * max(k, 1))(*[_pedge(a) for a in arrs])
+        counts = np.array([len(a) for a in arrs], dtype=np.int64)
+        self._c(LIB.scout_multi_stage(self._h, k, _p32(ids), ptrs, _p64(counts), None))
+
     def probe(self, batches, sched: Optional[dict] = None):
         """A round through Context.repair_probe semantics: (stats, variant_ms[3], features[24])."""
         k = len(batches)
@@ -664,3 +673,17 @@ class HybridGraph:
             self.close()
         except Exception:
             pass
+
+def run_fused_round(engines, sched: Optional[dict] = None) -> list:
+    """One round of several MultiEngines of distinct problems, each staged with stage(): their
+    merges, then ONE persistent kernel running all their repairs (scout_multi_run_all).
+    Returns each engine's stats; commit each engine as after round()."""
+    ne = len(engines)
+    hs = (C.c_void_p * max(ne, 1))(*[e._h for e in engines])
+    sts = (ScoutBatchStats * max(ne, 1))()
+    sd = ScoutSched()
+    for key, v in (sched or {}).items():
+        setattr(sd, key, v)
+    rc = LIB.scout_multi_run_all(ne, hs, C.byref(sd), sts)
+    _check(rc, LIB.scout_multi_context(engines[0]._h) if ne else None)
+    return [sts[i].as_dict() for i in range(ne)]
