@@ -67,13 +67,14 @@ typedef struct scout_sched {
     int32_t lanes_per_vertex; /* BFS expansion: most lanes that share one queue item (one
                                  chunk_log2-sized slice of a row) when a round has fewer
                                  items than warps: 32, 64, 128, 256 or 1024 (1-32 warps);
-                                 0 = as many warps as the item and the grid allow        */
+                                 0 = 64 (two warps), the best measured on a B200         */
     int64_t search_bound;     /* CC local-search bound (vertices); 0 = reference rule */
     int64_t search_limit;     /* CC: a class with more deletions left to search than this is
                                  recomputed instead (0 = 32; < 0 = always search)        */
     int32_t blocks_per_sm;    /* persistent repair kernels: resident blocks per SM (1..4;
                                  0 = as many as fit, at most 4)                          */
-    int32_t chunk_log2;       /* BFS queue item = 2^chunk_log2 row entries (8..13; 0 = 10) */
+    int32_t chunk_log2;       /* BFS queue item = 2^chunk_log2 row entries (8..13; 0 = 8,
+                                 the best measured on a B200)                            */
     int32_t prefetched;       /* 1: this call's edits (same count, no ops) are the batch given
                                  to the last scout_prefetch; the device copy that the previous
                                  scout_repair started is used instead of a new upload (when
@@ -353,8 +354,8 @@ int scout_host_free(void* p);
  * buffers live in one static device array of 8 MB that every GPU loading the library keeps
  * until the process exits, which bounds n to 1,048,576 vertices; larger graphs are refused
  * with SCOUT_E_CAPACITY. The first call on a device looks up that array's device address
- * (again after the device's context is recreated), so make the first call before any stream
- * capture. All calls share the array: calls that overlap on
+ * (again after the device's context is recreated). Every call waits for its stream, so it
+ * cannot be used while that stream is being captured. All calls share the array: calls that overlap on
  * the GPU (two host threads, or two streams) race and must be serialised by the caller.
  * No context is involved; errors are reported through scout_last_error(NULL). */
 int scout_bfs_levels_noalloc(const int64_t* d_off, const int32_t* d_adj, int64_t n, int32_t source,

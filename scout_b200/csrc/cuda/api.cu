@@ -320,7 +320,7 @@ static void fill_stats(scout_ctx* c, scout_batch_stats* st, int64_t launch0) {
 
 // Common prologue of a batch: validation, counters, classification + merge of the edits.
 // Tuning knobs of a call: persistent-kernel blocks per SM (1..4, 0 = as many as fit) and the
-// BFS queue item size (2^8 .. 2^13 row entries, 0 = 2^10).
+// BFS queue item size (2^8 .. 2^13 row entries, 0 = 2^8).
 static int apply_tuning(scout_ctx* c, const scout_sched& sd) {
     if (sd.blocks_per_sm < 0 || sd.blocks_per_sm > 4) return c->fail(SCOUT_E_INVALID, "blocks_per_sm must be 0..4");
     if (sd.chunk_log2 != 0 && (sd.chunk_log2 < 8 || sd.chunk_log2 > 13))
@@ -331,8 +331,10 @@ static int apply_tuning(scout_ctx* c, const scout_sched& sd) {
     if (sd.frontier < SCOUT_FRONTIER_AUTO || sd.frontier > SCOUT_FRONTIER_BITMAP)
         return c->fail(SCOUT_E_INVALID, "unknown frontier mode");
     c->tune_blocks_per_sm = sd.blocks_per_sm;
-    c->tune_chunk_log2 = sd.chunk_log2 ? sd.chunk_log2 : 10;
-    c->tune_share = lpv / 32;
+    // defaults: the autotuner's choice on a B200 (R-MAT scale 22 stream): 256-entry queue items,
+    // at most two warps sharing one
+    c->tune_chunk_log2 = sd.chunk_log2 ? sd.chunk_log2 : 8;
+    c->tune_share = (lpv ? lpv : 64) / 32;
     return SCOUT_OK;
 }
 

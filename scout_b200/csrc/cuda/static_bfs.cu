@@ -115,8 +115,7 @@ extern "C" int scout_bfs_levels_noalloc(const int64_t* d_off, const int32_t* d_a
     int32_t* scratch = nullptr;
     {
         // One-time set-up per device (and per context of it), with that device current: the
-        // device address of the static array. The first call on a device does it, so that call
-        // should come before any stream capture.
+        // device address of the static array, looked up by the first call on a device.
         std::lock_guard<std::mutex> g(g_setup_mu);
         const CUcontext cur = current_context();
         if (!g_scratch_ready[dev] || g_scratch_ctx[dev] != cur) {
