@@ -14,6 +14,12 @@
  *    (scout_last_error(NULL): last failure of scout_ctx_create on this thread).
  *  - Vertex ids are 0-indexed int32; adjacency offsets are int64.
  *  - Host buffers passed in are only read or written during the call; they may be pageable.
+ *    One exception: a page-locked batch given to scout_prefetch is read by the copy that the
+ *    next scout_repair call starts, so it stays unchanged until the repair that uses it.
+ *  - A repair call that fails after its batch was merged (a device error, a timeout, a
+ *    capacity error inside the repair) leaves that store's graph updated and its solution
+ *    unrepaired: reload the store (or recompute the solution) before the next batch. A fused
+ *    round (scout_multi_run_all) that fails does so for every engine of the round.
  *  - One controlling host thread per context. Contexts are independent (replicas).
  *  - No call drops work silently: a capacity overflow grows the buffer (within the HBM
  *    budget) or returns SCOUT_E_CAPACITY (the reference truncates and warns,
