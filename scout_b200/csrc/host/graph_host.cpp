@@ -223,32 +223,63 @@ void HGraph::neighbors_into(int32_t v, std::vector<int32_t>& out) const {
     out.resize((size_t)k);
 }
 
-// compact_flash_graph (flash_compactor.h:23-119) followed by remap + clear.
+// compact_flash_graph (flash_compactor.h:23-119) followed by remap + clear. The bytes are the
+// reference's (header, offsets, then every merged row in vertex order); the merged degrees
+// and rows are computed over the host threads (the scratchpad and the mapped base graph are
+// only read), the rows in windows of about COMPACT_WINDOW entries, each gathered into one
+// buffer at its final offsets and written with one call.
+constexpr uint64_t COMPACT_WINDOW = 1ull << 25;   // 32 M entries, 128 MB
+
 int HGraph::compact(const std::string& out_path) {
     const int64_t n = base.nodes();
     std::vector<uint64_t> nidx((size_t)n + 1);
-    nidx[0] = 0;
+    std::vector<int64_t> deg((size_t)n);
+    int64_t bad = n;
+#pragma omp parallel for schedule(static) reduction(min : bad)
     for (int64_t v = 0; v < n; v++) {
-        int64_t d = degree((int32_t)v);
-        if (d < 0) return host_fail(SCOUT_E_STATE, "negative merged degree at vertex " + std::to_string(v));
-        nidx[v + 1] = nidx[v] + (uint64_t)d;
+        deg[(size_t)v] = degree((int32_t)v);
+        if (deg[(size_t)v] < 0) bad = std::min(bad, v);
     }
+    if (bad < n) return host_fail(SCOUT_E_STATE, "negative merged degree at vertex " + std::to_string(bad));
+    nidx[0] = 0;
+    for (int64_t v = 0; v < n; v++) nidx[(size_t)v + 1] = nidx[(size_t)v] + (uint64_t)deg[(size_t)v];
     const std::string tmp = out_path + ".tmp." + std::to_string(getpid());
     FILE* out = std::fopen(tmp.c_str(), "wb");
     if (!out) return host_fail(SCOUT_E_IO, "could not open " + tmp + " for writing");
     int32_t n32 = (int32_t)n, sentinel = -1;
-    uint64_t ne = nidx[n];
+    uint64_t ne = nidx[(size_t)n];
     bool ok = fwrite_all(&n32, 4, 1, out) && fwrite_all(&sentinel, 4, 1, out) && fwrite_all(&ne, 8, 1, out) &&
               fwrite_all(nidx.data(), 8, nidx.size(), out);
-    std::vector<int32_t> row;
-    for (int64_t v = 0; ok && v < n; v++) {
-        neighbors_into((int32_t)v, row);
-        if ((uint64_t)row.size() != nidx[v + 1] - nidx[v]) {
+    std::vector<int32_t> buf;
+    for (int64_t v0 = 0; ok && v0 < n;) {
+        // the window: vertices [v0, v1) whose rows hold at most COMPACT_WINDOW entries (one
+        // vertex at least)
+        auto it = std::upper_bound(nidx.begin() + v0 + 1, nidx.end(), nidx[(size_t)v0] + COMPACT_WINDOW);
+        int64_t v1 = (int64_t)(it - nidx.begin()) - 1;
+        if (v1 <= v0) v1 = v0 + 1;
+        const uint64_t w0 = nidx[(size_t)v0];
+        buf.resize((size_t)(nidx[(size_t)v1] - w0));
+        int64_t mism = n;
+#pragma omp parallel reduction(min : mism)
+        {
+            std::vector<int32_t> row;
+#pragma omp for schedule(dynamic, 1024)
+            for (int64_t v = v0; v < v1; v++) {
+                neighbors_into((int32_t)v, row);
+                if ((uint64_t)row.size() != nidx[(size_t)v + 1] - nidx[(size_t)v]) {
+                    mism = std::min(mism, v);
+                } else if (!row.empty()) {
+                    std::memcpy(buf.data() + (nidx[(size_t)v] - w0), row.data(), row.size() * 4);
+                }
+            }
+        }
+        if (mism < n) {
             std::fclose(out);
             std::remove(tmp.c_str());
-            return host_fail(SCOUT_E_STATE, "degree mismatch at vertex " + std::to_string(v));
+            return host_fail(SCOUT_E_STATE, "degree mismatch at vertex " + std::to_string(mism));
         }
-        ok = fwrite_all(row.data(), 4, row.size(), out);
+        ok = fwrite_all(buf.data(), 4, buf.size(), out);
+        v0 = v1;
     }
     ok = ok && std::fflush(out) == 0 && fsync(fileno(out)) == 0;
     std::fclose(out);

@@ -208,3 +208,42 @@ def test_parallel_batch_parse_equals_serial(tmp_path):
     p.write_text("\n".join(lines) + "\n")
     got = sb.parse_batch_file(str(p), n)
     assert np.array_equal(got, np.array(want, dtype=np.int32).reshape(-1, 2))
+
+
+def test_compaction_spanning_rewrite_windows(tmp_path):
+    """The rewrite gathers rows over the host threads in windows of 2^25 entries: a graph of
+    more than one window, with toggles spread over the id range, compacts to the rows the
+    scratchpad held (unedited rows byte for byte the base's, edited rows in the reference's
+    order: base minus tombstones, then additions)."""
+    g = sb.gen_rmat(20, 18, seed=11)
+    off, adj = g.arrays()
+    assert off[-1] > (1 << 25)
+    src = tmp_path / "g.egr"
+    sb.write_egr(str(src), off, adj)
+    h = sb.HybridGraph(str(src))
+    n = len(off) - 1
+    rng = np.random.default_rng(5)
+    edited = set()
+    for u, v in rng.integers(0, n, size=(3000, 2)).tolist():
+        if u == v:
+            continue
+        if h.is_adjacent(u, v):
+            h.remove(u, v)
+            h.remove(v, u)
+        else:
+            h.insert(u, v)
+            h.insert(v, u)
+        edited.update((u, v))
+    want = {v: h.neighbors(v).copy() for v in edited}
+    out = tmp_path / "c.egr"
+    h.compact(str(out))
+    off2, adj2, _ = sb.read_egr(str(out))
+    deg, deg2 = np.diff(off), np.diff(off2)
+    mask = np.ones(n, dtype=bool)
+    mask[list(edited)] = False
+    assert np.array_equal(deg[mask], deg2[mask])
+    keep = np.repeat(mask, deg)
+    keep2 = np.repeat(mask, deg2)
+    assert np.array_equal(adj[keep], adj2[keep2])
+    for v, row in want.items():
+        assert np.array_equal(adj2[off2[v]:off2[v + 1]], row), f"row {v}"
