@@ -66,7 +66,7 @@ def test_fused_round_equals_streams_alone():
             truths.append(tr)
             me.seal()
         for j in range(4):
-            # round 2 leaves colouring out: a fused round takes any subset of the problems
+            # the third round leaves colouring out: a fused round takes any subset of the problems
             members = [pi for pi in range(4) if not (j == 2 and PROBLEMS[pi] == "coloring")]
             for pi in members:
                 engines[pi].stage([(sid, data[pi][sid][2][j]) for sid in range(3)])
