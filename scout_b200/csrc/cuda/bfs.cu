@@ -13,7 +13,8 @@
 //      inserted edges seed their endpoints (levels only ever decrease from here).
 //   C  relax rounds: atomicMin of level + 1 over the rows of every decreased vertex.
 // All three phases run in one cooperative launch separated by a bounded grid barrier; rows
-// longer than 1024 entries are split into 1024-entry chunks so a hub spreads over warps.
+// longer than one queue item (2^chunk_log2 entries, 256 by default) are split into items so a
+// hub spreads over warps.
 //
 // Two full traversals from the source replace the repair when the scheduler picks one
 // (mode 1: top-down with a queue frontier; mode 2: direction-optimizing, the frontier kept
